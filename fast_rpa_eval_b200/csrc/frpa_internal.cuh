@@ -1,0 +1,140 @@
+// Internal helpers shared by the frpa CUDA sources (not part of the C ABI).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdarg>
+#include <cstdint>
+#include <cstdio>
+#include <string>
+#include <vector>
+
+#include "frpa.h"
+
+namespace frpa {
+
+// ---------------------------------------------------------------- errors --
+
+// Records a failure for frpa_last_error()/frpa_last_error_message() and
+// returns the status so callers can `return fail(...)`.
+int fail(int status, const char *fmt, ...);
+void clear_error();
+
+#define FRPA_CUDA_TRY(call)                                                                      \
+  do {                                                                                           \
+    cudaError_t e_ = (call);                                                                     \
+    if (e_ != cudaSuccess)                                                                       \
+      return ::frpa::fail(FRPA_ERR_CUDA, "%s:%d: %s: %s", __FILE__, __LINE__, #call,             \
+                          cudaGetErrorString(e_));                                               \
+  } while (0)
+
+#define FRPA_CHECK_ARG(cond, ...)                                                                \
+  do {                                                                                           \
+    if (!(cond)) return ::frpa::fail(FRPA_ERR_INVALID, __VA_ARGS__);                             \
+  } while (0)
+
+#define FRPA_TRY(call)                                                                           \
+  do {                                                                                           \
+    int s_ = (call);                                                                             \
+    if (s_ != FRPA_OK) return s_;                                                                \
+  } while (0)
+
+// Launch-time check: configuration errors surface here, execution errors at
+// the next synchronising call.
+#define FRPA_LAUNCH_CHECK() FRPA_CUDA_TRY(cudaGetLastError())
+
+// ------------------------------------------------------------ device math --
+
+// Exactly rounded product and sum (no FMA contraction), used wherever the
+// reference's x86-64 arithmetic decides a branch (dist^2 vs radii).
+__device__ __forceinline__ double mul_rn(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ double add_rn(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ double sub_rn(double a, double b) { return __dsub_rn(a, b); }
+
+// 64-bit FP tensor-core MMA, m8n8k4 (A row-major 8x4, B col-major 4x8).
+// Fragments: a = A[lane>>2][lane&3], b = B[lane&3][lane>>2],
+// c/d = C[lane>>2][2*(lane&3) + {0,1}].
+__device__ __forceinline__ void dmma_8x8x4(double &d0, double &d1, double a, double b) {
+  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
+               : "+d"(d0), "+d"(d1)
+               : "d"(a), "d"(b));
+}
+
+// cp.async with zero fill: copies `src_bytes` (0 or the full size) and
+// zero-fills the rest of the destination.
+__device__ __forceinline__ void cp_async_8(void *smem_dst, const void *gmem_src, int src_bytes) {
+  unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem_dst));
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(s), "l"(gmem_src), "r"(src_bytes));
+}
+__device__ __forceinline__ void cp_async_16(void *smem_dst, const void *gmem_src, int src_bytes) {
+  unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem_dst));
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(s), "l"(gmem_src), "r"(src_bytes));
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(N));
+}
+
+inline int ceil_div(int a, int b) { return (a + b - 1) / b; }
+inline long long ceil_div_ll(long long a, long long b) { return (a + b - 1) / b; }
+
+// ------------------------------------------------------------ rho1 plan --
+
+// One unit of rho1 work: a point tile of one non-empty grid batch
+// (the reference's valid-batch list, device_data.cu:242-260, refined into
+// point tiles and ordered by decreasing cost for the persistent scheduler).
+struct Rho1WorkItem {
+  int batch;         // index into the caller's batch arrays
+  int nc;            // n_compute_c of the batch
+  int np;            // points in the batch
+  int p0;            // first point of this tile
+  int pn;            // points in this tile
+  int ib_off;        // offset of the batch's basis list in the compact list
+  int prefix;        // n_point_batches_prefix_sum[batch]
+  int pad_;
+  long long wave_off;  // i_batch_2_wave_offset[batch]
+};
+static_assert(sizeof(Rho1WorkItem) == 40, "work item layout");
+
+struct Rho1Plan {
+  int device = 0;
+  int T = 1;
+  int n_batches = 0;
+  int n_full_points = 0;
+  int n_basis = 0;
+  int n_max_batch_size = 0;
+  int n_max_compute = 0;
+  long long wave_len = 0;
+  int n_items = 0;
+  int n_valid_batches = 0;
+  long long n_valid_points = 0;  // points in batches with n_compute > 0
+  int wave_aligned16 = 0;        // every batch offset even -> 16-byte loads
+  // device copies
+  Rho1WorkItem *d_items = nullptr;
+  int *d_ib = nullptr;        // compact 1-based basis lists
+  int *d_map = nullptr;       // i_valid_point_2_i_full_points_map
+  int *d_counter = nullptr;   // persistent scheduler cursor
+  int grid_fp64 = 0;
+  // adjoint work list (batch, i tile, j tile, t), built with the plan
+  void *d_adj_items = nullptr;
+  int n_adj_items = 0;
+};
+
+int rho1_fp64_launch(const Rho1Plan &plan, int n_active, const double *wave, const double *gwave,
+                     const double *P1, const double *bias, const double *gbias, double *rho, double *grad,
+                     cudaStream_t stream);
+int rho1_fp64_grid(int device);
+
+int rho1_adjoint_launch_items(const Rho1Plan &plan, const void *d_items, int n_items, int n_active,
+                              const double *wave, const double *gwave, const double *g_rho, const double *g_grad,
+                              double *dP1, cudaStream_t stream);
+size_t rho1_adjoint_item_size();
+void rho1_adjoint_build_items(const int *nc_b, const int *np_b, const int *ib_off, const int *prefix,
+                              const long long *wave_off, int n_batches, int T, std::vector<unsigned char> *host);
+
+// ----------------------------------------------------------- sum-up plan --
+
+struct SumupPlan;  // defined in sumup.cu
+
+}  // namespace frpa

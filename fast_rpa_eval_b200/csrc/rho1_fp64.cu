@@ -1,0 +1,276 @@
+// Plain FP64 first-order density (rho1) and its gradient, one persistent
+// grouped launch over the plan's work list.
+//
+// Reference semantics (fast_rap_src_dfpt_gpu_eval/evaluate_first_order_rho.cpp:116-209):
+//   per non-empty grid batch b, perturbation t:
+//     P1c(i, j)   = P1(ib[i], ib[j], t)                       (gather, :149-159)
+//     work1       = P1c * phi                                 (GEMM,   :161-175)
+//     rho1(map p) = sum_i phi(i, p) work1(i, p) + bias(p, b, t)           (:177-207)
+//     grad(:,p,b,t) = 2 sum_i grad_phi(i, :, p) work1(i, p) - gbias(:, p, b, t)
+// The reference GPU path runs gather, a MAGMA vbatched DGEMM and a ddot kernel
+// as three launches with P1c and work1 round-tripping through HBM
+// (evaluate_first_order_rho.cu:282-360).  Here one CTA owns a (batch, point
+// tile) work item and fuses all three: P1c tiles are gathered straight into
+// shared memory, the contraction runs on the FP64 tensor-core MMA
+// (mma.sync m8n8k4 f64) with the accumulators in registers, and the epilogue
+// contracts each finished work1 tile against phi / grad phi, so work1 never
+// leaves the SM.  Per-point sums are reduced in a fixed order (registers ->
+// warp shuffles -> two shared-memory slots), so results are deterministic.
+#include "frpa_internal.cuh"
+
+namespace frpa {
+namespace {
+
+constexpr int BM = 64;       // rows (i_compute) per tile
+constexpr int BN = 64;       // points per tile
+constexpr int KC = 16;       // contraction chunk
+constexpr int STAGES = 3;    // cp.async pipeline depth
+constexpr int THREADS = 256; // 8 warps: 2 along M x 4 along N, warp tile 32 x 16
+constexpr int LDA = BM + 4;  // As[k][m]: stride = 4 (mod 16) doubles -> conflict-free fragment loads
+constexpr int LDB = KC + 4;  // Bs[n][k]
+constexpr int MAX_NC = FRPA_MAX_N_COMPUTE;
+
+struct Smem {
+  double A[STAGES][KC * LDA];
+  double B[STAGES][BN * LDB];
+  double red[2][4][BN];
+  int ib[MAX_NC];
+  int next;
+};
+
+__global__ void __launch_bounds__(THREADS, 2)
+    rho1_fp64_kernel(const Rho1WorkItem *__restrict__ items, int n_items, int *__restrict__ counter,
+                     const int *__restrict__ ib_all, const int *__restrict__ map, int T, int n_active, int n_basis,
+                     int n_full_points, int n_max_batch_size, int n_batches, const double *__restrict__ wave,
+                     const double *__restrict__ gwave, const double *__restrict__ P1,
+                     const double *__restrict__ bias, const double *__restrict__ gbias, double *__restrict__ rho,
+                     double *__restrict__ grad, int aligned16) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  Smem &S = *reinterpret_cast<Smem *>(smem_raw);
+  const int tid = threadIdx.x;
+  const int lane = tid & 31, warp = tid >> 5;
+  const int wm = warp >> 2, wn = warp & 3;
+  const int g = lane >> 2, q = lane & 3;
+  const long long nb2 = (long long)n_basis * n_basis;
+
+  for (;;) {
+    if (tid == 0) S.next = atomicAdd(counter, 1);
+    __syncthreads();
+    const int it = S.next;
+    if (it >= n_items) break;
+    const Rho1WorkItem W = items[it];
+    const int nc = W.nc, pn = W.pn;
+    const int ncp = (nc + 3) & ~3;
+    for (int i = tid; i < nc; i += THREADS) S.ib[i] = ib_all[W.ib_off + i] - 1;
+    __syncthreads();
+
+    const double *phi = wave + W.wave_off + (long long)W.p0 * ncp;
+    const double *gph = gwave + 3 * W.wave_off + 3LL * W.p0 * ncp;
+    const int nMt = (nc + BM - 1) / BM;
+    const int nKc = (nc + KC - 1) / KC;
+    const int steps = T * nMt * nKc;
+
+    auto load = [&](int s) {
+      const int kc = s % nKc;
+      const int rest = s / nKc;
+      const int mt = rest % nMt;
+      const int t = rest / nMt;
+      const int k0 = kc * KC, m0 = mt * BM;
+      double *As = S.A[s % STAGES];
+      double *Bs = S.B[s % STAGES];
+      const double *P = P1 + t * nb2;
+#pragma unroll
+      for (int j = 0; j < (BM * KC) / THREADS; ++j) {
+        const int e = tid + THREADS * j;
+        const int m = e & (BM - 1), k = e / BM;
+        const int gm = m0 + m, gk = k0 + k;
+        const bool ok = gm < nc && gk < nc;
+        const double *src = ok ? P + S.ib[gm] + (long long)S.ib[gk] * n_basis : P;
+        cp_async_8(&As[k * LDA + m], src, ok ? 8 : 0);
+      }
+      if (aligned16) {
+#pragma unroll
+        for (int j = 0; j < (BN * KC / 2) / THREADS; ++j) {
+          const int e = tid + THREADS * j;
+          const int kp = e & (KC / 2 - 1), n = e / (KC / 2);
+          const int gk = k0 + 2 * kp;
+          int bytes = 0;
+          if (n < pn) bytes = (gk + 1 < nc) ? 16 : (gk < nc ? 8 : 0);
+          const double *src = bytes ? phi + gk + (long long)n * ncp : phi;
+          cp_async_16(&Bs[n * LDB + 2 * kp], src, bytes);
+        }
+      } else {
+#pragma unroll
+        for (int j = 0; j < (BN * KC) / THREADS; ++j) {
+          const int e = tid + THREADS * j;
+          const int k = e & (KC - 1), n = e / KC;
+          const int gk = k0 + k;
+          const bool ok = n < pn && gk < nc;
+          cp_async_8(&Bs[n * LDB + k], ok ? phi + gk + (long long)n * ncp : phi, ok ? 8 : 0);
+        }
+      }
+    };
+
+    double acc[4][2][2];
+    double s_r[2][2], s_x[2][2], s_y[2][2], s_z[2][2];
+#pragma unroll
+    for (int a = 0; a < 4; ++a)
+#pragma unroll
+      for (int b = 0; b < 2; ++b) acc[a][b][0] = acc[a][b][1] = 0.0;
+#pragma unroll
+    for (int b = 0; b < 2; ++b)
+#pragma unroll
+      for (int h = 0; h < 2; ++h) s_r[b][h] = s_x[b][h] = s_y[b][h] = s_z[b][h] = 0.0;
+
+#pragma unroll
+    for (int s = 0; s < STAGES - 1; ++s) {
+      if (s < steps) load(s);
+      cp_async_commit();
+    }
+
+    for (int s = 0; s < steps; ++s) {
+      cp_async_wait<STAGES - 2>();
+      __syncthreads();
+      if (s + STAGES - 1 < steps) load(s + STAGES - 1);
+      cp_async_commit();
+
+      const int kc = s % nKc;
+      const int rest = s / nKc;
+      const int mt = rest % nMt;
+      const int t = rest / nMt;
+      const int k0 = kc * KC, m0 = mt * BM;
+      const double *As = S.A[s % STAGES];
+      const double *Bs = S.B[s % STAGES];
+      const int row_w = m0 + wm * 32;
+      const int col_w = wn * 16;
+#pragma unroll
+      for (int ks = 0; ks < KC / 4; ++ks) {
+        if (k0 + ks * 4 < nc) {
+          double a[4], b[2];
+#pragma unroll
+          for (int mi = 0; mi < 4; ++mi) a[mi] = As[(ks * 4 + q) * LDA + wm * 32 + mi * 8 + g];
+#pragma unroll
+          for (int ni = 0; ni < 2; ++ni) b[ni] = Bs[(col_w + ni * 8 + g) * LDB + ks * 4 + q];
+#pragma unroll
+          for (int mi = 0; mi < 4; ++mi)
+#pragma unroll
+            for (int ni = 0; ni < 2; ++ni)
+              if (row_w + mi * 8 < nc && col_w + ni * 8 < pn) dmma_8x8x4(acc[mi][ni][0], acc[mi][ni][1], a[mi], b[ni]);
+        }
+      }
+
+      if (kc == nKc - 1) {
+        // epilogue of one work1 tile: contract with phi and grad phi
+#pragma unroll
+        for (int mi = 0; mi < 4; ++mi) {
+          const int row = row_w + mi * 8 + g;
+          if (row < nc) {
+#pragma unroll
+            for (int ni = 0; ni < 2; ++ni)
+#pragma unroll
+              for (int h = 0; h < 2; ++h) {
+                const int col = col_w + ni * 8 + 2 * q + h;
+                if (col < pn) {
+                  const double w1 = acc[mi][ni][h];
+                  const long long pc = (long long)col * ncp;
+                  s_r[ni][h] += __ldg(phi + row + pc) * w1;
+                  const double *gp = gph + row + 3 * pc;
+                  s_x[ni][h] += __ldg(gp) * w1;
+                  s_y[ni][h] += __ldg(gp + ncp) * w1;
+                  s_z[ni][h] += __ldg(gp + 2 * ncp) * w1;
+                }
+              }
+          }
+#pragma unroll
+          for (int ni = 0; ni < 2; ++ni) acc[mi][ni][0] = acc[mi][ni][1] = 0.0;
+        }
+
+        if (mt == nMt - 1) {
+          // all rows of perturbation t done: reduce over rows and write
+#pragma unroll
+          for (int ni = 0; ni < 2; ++ni)
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+#pragma unroll
+              for (int off = 4; off < 32; off <<= 1) {
+                s_r[ni][h] += __shfl_xor_sync(0xffffffffu, s_r[ni][h], off);
+                s_x[ni][h] += __shfl_xor_sync(0xffffffffu, s_x[ni][h], off);
+                s_y[ni][h] += __shfl_xor_sync(0xffffffffu, s_y[ni][h], off);
+                s_z[ni][h] += __shfl_xor_sync(0xffffffffu, s_z[ni][h], off);
+              }
+            }
+          if (g == 0) {
+#pragma unroll
+            for (int ni = 0; ni < 2; ++ni)
+#pragma unroll
+              for (int h = 0; h < 2; ++h) {
+                const int col = col_w + ni * 8 + 2 * q + h;
+                S.red[wm][0][col] = s_r[ni][h];
+                S.red[wm][1][col] = s_x[ni][h];
+                S.red[wm][2][col] = s_y[ni][h];
+                S.red[wm][3][col] = s_z[ni][h];
+              }
+          }
+          __syncthreads();
+          if (tid < pn) {
+            const int p = W.p0 + tid;
+            const double r = S.red[0][0][tid] + S.red[1][0][tid];
+            const double gx = S.red[0][1][tid] + S.red[1][1][tid];
+            const double gy = S.red[0][2][tid] + S.red[1][2][tid];
+            const double gz = S.red[0][3][tid] + S.red[1][3][tid];
+            const long long bidx = p + (long long)n_max_batch_size * (W.batch + (long long)n_batches * t);
+            const long long gi = 3 * bidx;
+            grad[gi + 0] = gx * 2 - gbias[gi + 0];
+            grad[gi + 1] = gy * 2 - gbias[gi + 1];
+            grad[gi + 2] = gz * 2 - gbias[gi + 2];
+            if (t < n_active) rho[map[W.prefix + p] + (long long)n_full_points * t] = r + bias[bidx];
+          }
+#pragma unroll
+          for (int ni = 0; ni < 2; ++ni)
+#pragma unroll
+            for (int h = 0; h < 2; ++h) s_r[ni][h] = s_x[ni][h] = s_y[ni][h] = s_z[ni][h] = 0.0;
+          __syncthreads();
+        }
+      }
+    }
+    cp_async_wait<0>();
+    __syncthreads();
+  }
+}
+
+}  // namespace
+
+int rho1_fp64_grid(int device) {
+  static int cached[64] = {0};
+  if (device >= 0 && device < 64 && cached[device]) return cached[device];
+  const int smem = (int)sizeof(Smem);
+  if (cudaFuncSetAttribute(rho1_fp64_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) != cudaSuccess)
+    return 0;
+  int per_sm = 0, n_sm = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, rho1_fp64_kernel, THREADS, smem) != cudaSuccess) return 0;
+  if (cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, device) != cudaSuccess) return 0;
+  const int grid = (per_sm > 0 ? per_sm : 1) * n_sm;
+  if (device >= 0 && device < 64) cached[device] = grid;
+  return grid;
+}
+
+int rho1_fp64_launch(const Rho1Plan &plan, int n_active, const double *wave, const double *gwave, const double *P1,
+                     const double *bias, const double *gbias, double *rho, double *grad, cudaStream_t stream) {
+  // evaluate_first_order_rho.cpp:113-114 zeroes both outputs before the batch loop
+  FRPA_CUDA_TRY(cudaMemsetAsync(rho, 0, sizeof(double) * (size_t)plan.n_full_points * plan.T, stream));
+  FRPA_CUDA_TRY(cudaMemsetAsync(
+      grad, 0, sizeof(double) * 3 * (size_t)plan.n_max_batch_size * plan.n_batches * plan.T, stream));
+  if (plan.n_items == 0) return FRPA_OK;
+  FRPA_CUDA_TRY(cudaMemsetAsync(plan.d_counter, 0, sizeof(int), stream));
+  int grid = plan.grid_fp64 > 0 ? plan.grid_fp64 : rho1_fp64_grid(plan.device);
+  if (grid <= 0) return fail(FRPA_ERR_CUDA, "rho1_fp64: occupancy query failed");
+  if (grid > plan.n_items) grid = plan.n_items;
+  rho1_fp64_kernel<<<grid, THREADS, sizeof(Smem), stream>>>(
+      plan.d_items, plan.n_items, plan.d_counter, plan.d_ib, plan.d_map, plan.T, n_active, plan.n_basis,
+      plan.n_full_points, plan.n_max_batch_size, plan.n_batches, wave, gwave, P1, bias, gbias, rho, grad,
+      plan.wave_aligned16);
+  FRPA_LAUNCH_CHECK();
+  return FRPA_OK;
+}
+
+}  // namespace frpa

@@ -485,7 +485,7 @@ def make_sumup_problem(
     L = l_pot_max
     L2 = (L + 1) ** 2
     lma = L + 1
-    index_cc, cc, n_cc, ijk_max = tables.multipole_tables(lma)
+    index_cc, cc, n_cc, ijk_max = (np.array(a, order="F", copy=True) for a in tables.multipole_tables(lma))
     atoms = place_atoms(n_atoms, rng, density=density, min_dist=min_atom_dist)
     box = (n_atoms / density) ** (1.0 / 3.0)
     n_full = n_points + extra_full_points

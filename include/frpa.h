@@ -1,0 +1,279 @@
+/*
+ * frpa: B200-native (sm_100a) DFPT grid hot paths behind a C ABI.
+ *
+ *  1. The first-order density rho1 and its gradient
+ *     (evaluate_first_order_rho_reduce_memory_c_v3_batches_atoms_).
+ *  2. The Hartree potential sum-up from atomic multipoles
+ *     (sum_up_whole_potential_c_v3_atoms_full_points_j_atom_tile_).
+ *
+ * Three layers:
+ *  - Reference drop-ins: the reference's own entry-point names, argument lists
+ *    and array layouts (Fortran column-major, 1-based basis / species / centre
+ *    indices, 0-based full-point indices).  They take HOST pointers.  The void
+ *    ones report failures through frpa_last_error() instead of exit(1).
+ *    Citations are to the reference project kzwrime/fast_rpa_eval,
+ *    directory fast_rap_src_dfpt_gpu_eval/.
+ *  - The reference's device session (init_dfpt_device_info / _data and the
+ *    *_cu_host_ twins), which keeps the constant arrays resident on the GPU.
+ *  - Plans: an explicit, re-entrant, stream-ordered API on DEVICE pointers
+ *    (what the Python bindings, the benchmarks and CUDA-graph capture use).
+ *
+ * The reference fixes the perturbation tile size ATOM_TILE_SIZE at compile
+ * time (setting.h:19-21); here it is a runtime setting (default 1).
+ * Everything is FP64 except the optional split-BF16 rho1 contraction.
+ */
+#ifndef FRPA_H
+#define FRPA_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ------------------------------------------------------------------ limits */
+#define FRPA_MAX_N_COMPUTE 2048 /* n_compute_c per batch */
+#define FRPA_MAX_ATOM_TILE 64   /* ATOM_TILE_SIZE */
+#define FRPA_SUMUP_MAX_L 8      /* l_pot_max */
+
+/* ---------------------------------------------------------------- status */
+enum {
+  FRPA_OK = 0,
+  FRPA_ERR_INVALID = 1,     /* bad argument or inconsistent input arrays */
+  FRPA_ERR_CUDA = 2,        /* CUDA runtime error (message has the details) */
+  FRPA_ERR_NO_SESSION = 3,  /* *_cu_host_ called before init_dfpt_device_data */
+  FRPA_ERR_OOM = 4,         /* device allocation failed */
+  FRPA_ERR_UNSUPPORTED = 5, /* valid input outside what this build implements */
+  FRPA_ERR_DEVICE_INPUT = 6 /* a device-side input check failed (see message) */
+};
+
+/* Status of the last failing call on this thread (FRPA_OK if none since the
+ * last frpa_clear_error), and its message. */
+int frpa_last_error(void);
+const char *frpa_last_error_message(void);
+void frpa_clear_error(void);
+int frpa_version(void);
+
+/* ATOM_TILE_SIZE for the reference drop-ins (setting.h:19-21), 1..64. */
+int frpa_set_atom_tile_size(int T);
+int frpa_get_atom_tile_size(void);
+
+/* rho1 contraction mode used by the reference drop-ins. */
+enum { FRPA_RHO1_FP64 = 0, FRPA_RHO1_SPLIT_BF16 = 1 };
+int frpa_set_rho1_mode(int mode);
+int frpa_get_rho1_mode(void);
+
+/* =========================================================================
+ * Reference drop-ins (host pointers)
+ * ======================================================================= */
+
+/* Replaces evaluate_first_order_rho_reduce_memory_c_v3_batches_atoms_
+ * (evaluate_first_order_rho.h:3-35, CPU implementation evaluate_first_order_rho.cpp:12-210).
+ * Same arguments and layouts; computes on the GPU (uploads everything, runs,
+ * downloads first_order_rho and first_order_gradient_rho, which are zeroed and
+ * then written as in the reference).  basis_atom, partition_tab and
+ * density_matrix are accepted and unused, as in the reference. */
+void evaluate_first_order_rho_reduce_memory_c_v3_batches_atoms_(
+    int *n_my_batches_work, int *j_atom_begin, int *j_atom_end, int *j_coord, int *n_full_points, int *n_basis,
+    int *n_atoms, int *n_max_compute_ham, int *n_centers_basis_I, int *n_max_batch_size, int *batch_sizes,
+    int *n_point_batches, int *n_point_batches_prefix_sum, int *i_valid_point_2_i_full_points_map,
+    int *n_compute_c_batches, int *i_basis_batches, int *atom_valid_n_compute_c_batches, int *i_batch_2_wave_offset,
+    double *wave_batches_compress, double *gradient_wave_batches_compress, double *first_order_density_matrix,
+    double *first_order_rho, double *first_order_rho_bias_part2, double *first_order_gradient_rho,
+    double *first_order_gradient_rho_bias_batches_atoms, int *basis_atom, double *partition_tab,
+    double *density_matrix);
+
+/* Replaces evaluate_first_order_rho_reduce_memory_c_v3_batches_atoms_cu_host_
+ * (evaluate_first_order_rho.h:37-69, evaluate_first_order_rho.cu:188-371).
+ * Uses the arrays made resident by init_dfpt_device_data; per call it uploads
+ * the changeable inputs first_order_density_matrix, first_order_rho_bias_part2
+ * and first_order_gradient_rho_bias_batches_atoms from the host pointers,
+ * computes, and downloads first_order_rho and first_order_gradient_rho (the
+ * reference's host-copy mode, evaluate_first_order_rho.cu:259-263,363-367).
+ * The outputs also stay resident (frpa_session_rho1_device_outputs). */
+void evaluate_first_order_rho_reduce_memory_c_v3_batches_atoms_cu_host_(
+    int *n_my_batches_work, int *j_atom_begin, int *j_atom_end, int *j_coord, int *n_full_points, int *n_basis,
+    int *n_atoms, int *n_max_compute_ham, int *n_centers_basis_I, int *n_max_batch_size, int *batch_sizes,
+    int *n_point_batches, int *n_point_batches_prefix_sum, int *i_valid_point_2_i_full_points_map,
+    int *n_compute_c_batches, int *i_basis_batches, int *atom_valid_n_compute_c_batches, int *i_batch_2_wave_offset,
+    double *wave_batches_compress, double *gradient_wave_batches_compress, double *first_order_density_matrix,
+    double *first_order_rho, double *first_order_rho_bias_part2, double *first_order_gradient_rho,
+    double *first_order_gradient_rho_bias_batches_atoms, int *basis_atom, double *partition_tab,
+    double *density_matrix);
+
+/* Replaces sum_up_whole_potential_c_v3_atoms_full_points_j_atom_tile_
+ * (sum_up_whole_potential.h:3-48, sum_up_whole_potential.cpp:195-529).
+ * Accumulates into delta_v_hartree (n_full_points, ATOM_TILE_SIZE).
+ * l_pot_max <= 8 (the reference's own near field stops at 6). */
+void sum_up_whole_potential_c_v3_atoms_full_points_j_atom_tile_(
+    const int *j_atom_begin, const int *j_atom_end, const int *n_full_points, const int *l_max_analytic_multipole,
+    const int *index_cc_dim_0, const int *n_valid_points, const int *l_pot_max, const int *n_max_radial,
+    const int *n_hartree_grid, const int *n_centers, const int *n_centers_hartree_potential, const int *n_atoms,
+    const int *hartree_force_l_add, const int *n_species, const int *n_radial, const int *species,
+    const int *species_center, const int *l_hartree_max_far_distance, const int *i_valid_point_2_i_full_points_map,
+    const double *coord_points, const double *multipole_radius_sq, const double *outer_potential_radius,
+    const double *multipole_moments, const double *current_delta_v_hart_part_spl_tile, const int *l_hartree,
+    const int *n_grid, const int *n_cc_lm_ijk, const int *centers_hartree_potential, const int *center_to_atom,
+    const int *index_cc, const int *index_ijk_max_cc, const double *cc, const double *coords_center,
+    const double *r_grid_min, const double *log_r_grid_inc, const double *scale_radial, const double *partition_tab,
+    double *delta_v_hartree);
+
+/* Replaces sum_up_whole_potential_c_v3_atoms_full_points_j_atom_tile_cu_host_
+ * (sum_up_whole_potential.h:50-95, sum_up_whole_potential.cu:548-769; C++
+ * linkage there, C linkage here).  Scalars by value.  Constant arrays come from
+ * the session; the changeable ones (l_hartree_max_far_distance,
+ * multipole_radius_sq, outer_potential_radius, multipole_moments, the spline
+ * table and delta_v_hartree) are uploaded from the host pointers, and
+ * delta_v_hartree is downloaded again (sum_up_whole_potential.cu:641-647,768-769). */
+void sum_up_whole_potential_c_v3_atoms_full_points_j_atom_tile_cu_host_(
+    int j_atom_begin, int j_atom_end, int n_full_points, int l_max_analytic_multipole, int index_cc_dim_0,
+    int n_valid_points, int l_pot_max, int n_max_radial, int n_hartree_grid, int n_centers,
+    int n_centers_hartree_potential, int n_atoms, int hartree_force_l_add, int n_species, const int *n_radial,
+    const int *species, const int *species_center, const int *l_hartree_max_far_distance,
+    const int *i_valid_point_2_i_full_points_map, const double *coord_points, const double *multipole_radius_sq,
+    const double *outer_potential_radius, const double *multipole_moments,
+    const double *current_delta_v_hart_part_spl_tile, const int *l_hartree, const int *n_grid,
+    const int *n_cc_lm_ijk, const int *centers_hartree_potential, const int *center_to_atom, const int *index_cc,
+    const int *index_ijk_max_cc, const double *cc, const double *coords_center, const double *r_grid_min,
+    const double *log_r_grid_inc, const double *scale_radial, const double *partition_tab,
+    double *delta_v_hartree);
+
+/* Replaces init_dfpt_device_info (device.hpp:191, device.cu:7-33): selects
+ * device 0 (or $FRPA_DEVICE) and creates the session stream. */
+void init_dfpt_device_info(void);
+/* Replaces free_dfpt_device_info (device.hpp:192, device.cu:35-38). */
+void free_dfpt_device_info(void);
+
+/* Replaces init_dfpt_device_data (device_data.hpp:159-225, device_data.cu:10-361):
+ * validates and uploads the constant arrays once, builds the rho1 work list
+ * (the reference's valid-batch list and per-tile GEMM metadata,
+ * device_data.cu:242-300) and the sum-up plan. */
+void init_dfpt_device_data(
+    int *n_my_batches_work, int *n_full_points, int *n_valid_points, int *n_basis, int *n_atoms,
+    int *n_max_compute_ham, int *n_centers_basis_I, int *n_max_batch_size, int *l_pot_max, int *n_max_radial,
+    int *n_hartree_grid, int *n_centers, int *n_centers_hartree_potential, int *hartree_force_l_add, int *n_species,
+    int *l_max_analytic_multipole, int *index_cc_dim_0, int *basis_atom, int *batch_sizes, int *n_point_batches,
+    int *n_point_batches_prefix_sum, int *i_valid_point_2_i_full_points_map, int *n_compute_c_batches,
+    int *i_basis_batches, int *atom_valid_n_compute_c_batches, int *i_batch_2_wave_offset,
+    double *wave_batches_compress, double *gradient_wave_batches_compress, double *density_matrix, int *n_radial,
+    int *species, int *species_center, double *coord_points, int *l_hartree, int *n_grid, int *n_cc_lm_ijk,
+    int *centers_hartree_potential, int *center_to_atom, int *index_cc, int *index_ijk_max_cc, double *cc,
+    double *coords_center, double *r_grid_min, double *log_r_grid_inc, double *scale_radial, double *partition_tab,
+    double *first_order_density_matrix, double *first_order_rho, double *first_order_rho_bias_part2,
+    double *first_order_gradient_rho, double *first_order_gradient_rho_bias_batches_atoms,
+    int *l_hartree_max_far_distance, double *multipole_radius_sq, double *outer_potential_radius,
+    double *multipole_moments, double *current_delta_v_hart_part_spl_tile, double *delta_v_hartree);
+
+/* Replaces free_dfpt_device_data (device_data.hpp:227, device_data.cu:363-431). */
+void free_dfpt_device_data(void);
+
+/* Device addresses of the session's resident rho1 outputs (after a
+ * *_cu_host_ call), for callers that keep working on the GPU. */
+int frpa_session_rho1_device_outputs(double **first_order_rho, double **first_order_gradient_rho);
+
+/* =========================================================================
+ * Plans: device pointers, explicit stream (cudaStream_t passed as void *)
+ * ======================================================================= */
+
+typedef struct frpa_rho1_plan frpa_rho1_plan;
+
+/* Batch metadata for rho1 (host arrays, reference layouts).  The plan builds
+ * the device work list: valid batches (n_compute_c > 0) split into point tiles
+ * and ordered by cost for the persistent grouped kernels. */
+typedef struct {
+  int atom_tile_size; /* T */
+  int n_my_batches_work;
+  int n_full_points;
+  int n_basis;
+  int n_centers_basis_I;
+  int n_max_batch_size;
+  const int *n_point_batches;                   /* (n_batches) */
+  const int *n_point_batches_prefix_sum;        /* (n_batches + 1) */
+  const int *i_valid_point_2_i_full_points_map; /* (>= prefix[n_batches]) 0-based */
+  const int *n_compute_c_batches;               /* (n_batches) */
+  const int *i_basis_batches;                   /* (n_centers_basis_I, n_batches) 1-based */
+  const int *i_batch_2_wave_offset;             /* (n_batches + 1) */
+  long long wave_alloc_len;                     /* elements available in the wave array
+                                                   (0: trust i_batch_2_wave_offset) */
+} frpa_rho1_desc;
+
+int frpa_rho1_plan_create(frpa_rho1_plan **plan, const frpa_rho1_desc *desc);
+int frpa_rho1_plan_destroy(frpa_rho1_plan *plan);
+/* Work-list statistics: [n_items, n_valid_batches, n_valid_points]. */
+int frpa_rho1_plan_info(const frpa_rho1_plan *plan, long long *info3);
+
+/* rho1 and grad rho1 for perturbations t < T; rho1 is written for
+ * t < n_active = j_atom_end - j_atom_begin + 1 (evaluate_first_order_rho.cpp:202-207).
+ * wave (n elements), gradient_wave (3n), P1 (n_basis, n_basis, T),
+ * bias (n_max_batch_size, n_batches, T), gbias (3, n_max_batch_size, n_batches, T);
+ * outputs rho (n_full_points, T) and grad (3, n_max_batch_size, n_batches, T). */
+int frpa_rho1_execute(const frpa_rho1_plan *plan, int mode, int n_active, const double *wave,
+                      const double *gradient_wave, const double *P1, const double *bias, const double *gbias,
+                      double *rho, double *grad, void *stream);
+
+/* Adjoint: dP1 (n_basis, n_basis, T) += d(sum g_rho . rho1 + sum g_grad . grad)/dP1.
+ * g_rho (n_full_points, T) or NULL, g_grad like grad or NULL.  dP1 is NOT zeroed. */
+int frpa_rho1_adjoint_p1(const frpa_rho1_plan *plan, int n_active, const double *wave, const double *gradient_wave,
+                         const double *g_rho, const double *g_grad, double *dP1, void *stream);
+
+typedef struct frpa_sumup_plan frpa_sumup_plan;
+
+/* Constant sum-up inputs (host arrays, reference layouts and meanings). */
+typedef struct {
+  int atom_tile_size;
+  int n_full_points, l_max_analytic_multipole, index_cc_dim_0, n_valid_points;
+  int l_pot_max, n_hartree_grid, n_centers, n_centers_hartree_potential, n_atoms, hartree_force_l_add, n_species;
+  const int *species, *species_center, *i_valid_point_2_i_full_points_map;
+  const double *coord_points;
+  const int *l_hartree, *n_grid, *n_cc_lm_ijk, *centers_hartree_potential, *center_to_atom, *index_cc,
+      *index_ijk_max_cc;
+  const double *cc, *coords_center, *r_grid_min, *log_r_grid_inc;
+} frpa_sumup_desc;
+
+int frpa_sumup_plan_create(frpa_sumup_plan **plan, const frpa_sumup_desc *desc);
+int frpa_sumup_plan_destroy(frpa_sumup_plan *plan);
+/* 1 if the Kelvin-polynomial far-field path applies (identity
+ * centers_hartree_potential and a homogeneous multipole table). */
+int frpa_sumup_plan_fast(const frpa_sumup_plan *plan);
+
+/* Accumulates into delta_v (n_full_points, T) for t < n_active.  Per-call
+ * inputs: l_hartree_max_far_distance (n_atoms, T), multipole_radius_sq
+ * (n_atoms, T), outer_potential_radius (l_pot_max+1, n_atoms, T),
+ * multipole_moments ((l_pot_max+1)^2, n_atoms, T), spline
+ * ((l_pot_max+1)^2, 2, n_hartree_grid, n_atoms, T).  branch_codes (optional,
+ * (n_valid, n_centers_hartree_potential, T) bytes): 0 skipped, 1 + l_atom_max
+ * near field, 16 + l_atom_max far field.  flags: bit 0 forces the generic
+ * (reference table loop) kernel. */
+int frpa_sumup_execute(const frpa_sumup_plan *plan, int n_active, int flags, const int *l_hartree_max_far_distance,
+                       const double *multipole_radius_sq, const double *outer_potential_radius,
+                       const double *multipole_moments, const double *spline, double *delta_v,
+                       unsigned char *branch_codes, void *stream);
+
+/* Adjoint of the sum-up with respect to the multipole moments:
+ * dQ ((l_pot_max+1)^2, n_atoms, T) = d(sum_p g(p, t) delta_v(p, t))/dQ, zeroed
+ * first.  Needs the fast path (frpa_sumup_plan_fast). */
+int frpa_sumup_adjoint_q(const frpa_sumup_plan *plan, int n_active, const int *l_hartree_max_far_distance,
+                         const double *multipole_radius_sq, const double *outer_potential_radius,
+                         const double *multipole_moments, const double *g, double *dQ, void *stream);
+
+/* Reads and clears the device-side input flags of the last executions
+ * (bit 0: an l_hartree_max_far_distance entry outside 0..l_pot_max, clamped). */
+int frpa_sumup_device_flags(const frpa_sumup_plan *plan, int *flags);
+
+/* =========================================================================
+ * Synthetic workload generator (benchmarks and tests)
+ * ======================================================================= */
+
+/* Fills wave / gradient_wave (device) with Gaussian basis functions
+ * phi = R_lm(r - R_A) exp(-alpha |r - R_A|^2) at the batches' points.
+ * points: device (3, n_valid) in valid-point order; basis_atom (0-based),
+ * basis_l, basis_m, basis_alpha: host (n_basis); atoms: host (3, n_atoms).
+ * Rows n_compute..n_compute_padding-1 are set to pad_value. */
+int frpa_synth_basis_values(const frpa_rho1_desc *desc, const double *points, int n_atoms, const double *atoms,
+                            const int *basis_atom, const int *basis_l, const int *basis_m, const double *basis_alpha,
+                            double pad_value, double *wave, double *gradient_wave, void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* FRPA_H */
