@@ -269,41 +269,55 @@ def make_rho1_problem(
 
     # points of each batch: uniform in a ball around a random atom
     centre_atom = rng.integers(0, n_atoms, n_batches)
-    pts_list = []
-    for b in range(n_batches):
-        u = rng.normal(size=(npts[b], 3))
-        u /= np.linalg.norm(u, axis=1, keepdims=True)
-        r = point_radius * rng.uniform(0, 1, npts[b]) ** (1.0 / 3.0)
-        pts_list.append(atoms[centre_atom[b]] + u * r[:, None])
+    tot = int(npts.sum())
+    u = rng.normal(size=(tot, 3))
+    u /= np.linalg.norm(u, axis=1, keepdims=True)
+    r = point_radius * rng.uniform(0, 1, tot) ** (1.0 / 3.0)
+    owner = np.repeat(np.arange(n_batches), npts)
+    all_pts = atoms[centre_atom[owner]] + u * r[:, None]
+    starts = np.zeros(n_batches + 1, np.int64)
+    starts[1:] = np.cumsum(npts)
+    pts_list = [all_pts[starts[b]:starts[b + 1]] for b in range(n_batches)]
 
     # n_compute selection: the strongest functions over the batch
     atom_of = basis.atom
-    ib_list = []
-    for b in range(n_batches):
-        nc = int(ncs[b])
-        if nc == 0:
-            ib_list.append(np.zeros(0, np.int64))
-            continue
-        pts = pts_list[b]
-        if exact_selection:
-            phi, _ = eval_basis(basis, np.arange(n_basis), atoms, pts)
+    ib_list = [None] * n_batches
+    if exact_selection:
+        for b in range(n_batches):
+            nc = int(ncs[b])
+            if nc == 0:
+                ib_list[b] = np.zeros(0, np.int64)
+                continue
+            phi, _ = eval_basis(basis, np.arange(n_basis), atoms, pts_list[b])
             score = np.max(np.abs(phi), axis=1)
-        else:
-            c = pts.mean(axis=0)
-            rad = np.max(np.linalg.norm(pts - c, axis=1))
-            d_atom = np.linalg.norm(atoms - c, axis=1)
-            near = np.argsort(d_atom)[: max(8, min(n_atoms, 4 * nc // max(1, n_basis // n_atoms) + 8))]
-            cand = np.nonzero(np.isin(atom_of, near))[0]
-            d = d_atom[atom_of[cand]]
-            lo, hi = np.maximum(d - rad, 0.0), d + rad
-            lv = basis.l[cand].astype(np.float64)
-            al = basis.alpha[cand]
-            rstar = np.clip(np.sqrt(lv / (2 * al)), lo, hi)
-            score_c = rstar**lv * np.exp(-al * rstar * rstar)
-            score = np.full(n_basis, -1.0)
-            score[cand] = score_c
-        top = np.argpartition(-score, nc - 1)[:nc]
-        ib_list.append(np.sort(top))
+            ib_list[b] = np.sort(np.argpartition(-score, nc - 1)[:nc])
+    else:
+        # radial envelope max of r^l exp(-a r^2) over the batch ball, for the
+        # functions of the atoms nearest the batch centre
+        fpa = max(1, n_basis // n_atoms)
+        k_near = int(min(n_atoms, max(8, 4 * int(ncs.max()) // fpa + 8)))
+        funcs_of_atom = np.arange(n_basis).reshape(n_atoms, fpa) if n_basis == n_atoms * fpa else None
+        chunk = 2048
+        for b0 in range(0, n_batches, chunk):
+            b1 = min(n_batches, b0 + chunk)
+            c = atoms[centre_atom[b0:b1]]
+            d_atom = np.linalg.norm(c[:, None, :] - atoms[None, :, :], axis=2)
+            near = np.argpartition(d_atom, k_near - 1, axis=1)[:, :k_near]
+            for bi, b in enumerate(range(b0, b1)):
+                nc = int(ncs[b])
+                if nc == 0:
+                    ib_list[b] = np.zeros(0, np.int64)
+                    continue
+                cand = funcs_of_atom[near[bi]].ravel() if funcs_of_atom is not None else np.nonzero(np.isin(atom_of, near[bi]))[0]
+                d = d_atom[bi, atom_of[cand]]
+                lo, hi = np.maximum(d - point_radius, 0.0), d + point_radius
+                lv = basis.l[cand].astype(np.float64)
+                al = basis.alpha[cand]
+                rstar = np.clip(np.sqrt(lv / (2 * al)), lo, hi)
+                score_c = rstar**lv * np.exp(-al * rstar * rstar)
+                nc = min(nc, len(cand))
+                ncs[b] = nc
+                ib_list[b] = np.sort(cand[np.argpartition(-score_c, nc - 1)[:nc]])
 
     n_max_compute_ham = int(max(1, ncs.max()))
     n_centers_basis_I = n_basis if n_basis * n_batches <= 50_000_000 else n_max_compute_ham
@@ -357,13 +371,16 @@ def make_rho1_problem(
         mask = np.zeros((n_atoms, n_atoms), bool)
         for b in range(n_batches):
             at = np.unique(atom_of[ib_list[b]])
-            mask[np.ix_(at, at)] = True
+            mask[at[:, None], at[None, :]] = True
         scale = math.sqrt(max(1.0, float(ncs[ncs > 0].mean())))
         full_mask = mask[np.ix_(atom_of, atom_of)]
         for t in range(T):
-            a = rng.normal(size=(n_basis, n_basis)) / scale
-            a = np.triu(a) + np.triu(a, 1).T
-            P1[:, :, t] = np.where(full_mask, a, 0.0)
+            a = rng.standard_normal(size=(n_basis, n_basis))
+            a *= 1.0 / scale
+            a = np.triu(a)
+            a += np.triu(a, 1).T
+            a[~full_mask] = 0.0
+            P1[:, :, t] = a
 
     nmb = int(npts.max()) if n_batches else 1
     if with_bias:
