@@ -324,7 +324,9 @@ class Session:
     init_dfpt_device_data, the *_cu_host_ twins, free_*.  Holds references to
     every host array passed in so they outlive the calls."""
 
-    def __init__(self, rho_prob, sumup_prob=None):
+    def __init__(self, rho_prob, sumup_prob=None, wave=None, gradient_wave=None):
+        """``wave`` / ``gradient_wave`` (device tensors) replace the problem's
+        host arrays; the session then uses them in place."""
         self.rho_prob, self.sumup_prob = rho_prob, sumup_prob
         T = rho_prob.T
         if sumup_prob is not None and sumup_prob.T != T:
@@ -359,7 +361,8 @@ class Session:
             k.i(r.basis_atom), k.i(r.batch_sizes), k.i(r.n_point_batches), k.i(r.n_point_batches_prefix_sum),
             k.i(r.i_valid_point_2_i_full_points_map if s is None else s.i_valid_point_2_i_full_points_map),
             k.i(r.n_compute_c_batches), k.i(r.i_basis_batches), k.i(r.atom_valid_n_compute_c_batches),
-            k.i(r.i_batch_2_wave_offset), k.d(r.wave), k.d(r.gradient_wave), k.d(dm),
+            k.i(r.i_batch_2_wave_offset), _ptr(wave) if wave is not None else k.d(r.wave),
+            _ptr(gradient_wave) if gradient_wave is not None else k.d(r.gradient_wave), k.d(dm),
             g("n_radial", "i"), g("species", "i"), g("species_center", "i"), g("coord_points", "d"),
             g("l_hartree", "i"), g("n_grid", "i"), g("n_cc_lm_ijk", "i"), g("centers_hartree_potential", "i"),
             g("center_to_atom", "i"), g("index_cc", "i"), g("index_ijk_max_cc", "i"), g("cc", "d"),
@@ -438,3 +441,12 @@ def _host_ptr(a, keep: _Keep, writable: bool = False):
     if writable:
         raise ValueError("output arrays must be contiguous float64")
     return keep.d(a)
+
+
+def probe_fp64_tflops(kind: str = "mma") -> float:
+    """Measured FP64 throughput of the current device: 'mma' (tensor pipe,
+    m8n8k4 f64) or 'fma' (DFMA pipe)."""
+    v = ctypes.c_double(0.0)
+    fn = lib().frpa_probe_fp64_mma_tflops if kind == "mma" else lib().frpa_probe_fp64_fma_tflops
+    check(fn(ctypes.byref(v), c_void_p(0)))
+    return v.value

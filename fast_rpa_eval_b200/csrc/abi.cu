@@ -260,6 +260,7 @@ struct Session {
   Rho1Plan *rho = nullptr;
   int n_batches = 0, n_full_points = 0, n_basis = 0, n_max_batch_size = 0;
   double *wave = nullptr, *gwave = nullptr;
+  bool borrowed_wave = false;  // wave arrays were already device memory
   double *P1 = nullptr, *bias = nullptr, *gbias = nullptr, *out_rho = nullptr, *out_grad = nullptr;
   // sum-up
   SumupPlan *sumup = nullptr;
@@ -273,6 +274,8 @@ Session g_session;
 void session_free_data(Session &S) {
   if (S.rho) rho1_plan_free(S.rho);
   if (S.sumup) sumup_plan_free(S.sumup);
+  if (S.borrowed_wave) S.wave = S.gwave = nullptr;
+  S.borrowed_wave = false;
   void *ptrs[] = {S.wave, S.gwave, S.P1, S.bias, S.gbias, S.out_rho, S.out_grad, S.lhmfd, S.mrs, S.opr, S.Q, S.spline, S.dv};
   for (void *p : ptrs)
     if (p) cudaFree(p);
@@ -681,14 +684,29 @@ void init_dfpt_device_data(
     if (cudaMalloc(p, std::max<size_t>(bytes, 256)) != cudaSuccess)
       fail(FRPA_ERR_OOM, "init_dfpt_device_data: allocation of %zu bytes failed", bytes);
   };
-  alloc((void **)&S.wave, sizeof(double) * wl);
-  alloc((void **)&S.gwave, sizeof(double) * 3 * wl);
+  // Wave arrays that are already device memory of this GPU (e.g. computed
+  // there by the caller) are used in place instead of copied; the caller
+  // keeps them alive until free_dfpt_device_data.
+  cudaPointerAttributes wa{}, ga{};
+  const bool dev_wave = cudaPointerGetAttributes(&wa, wave_batches_compress) == cudaSuccess &&
+                        cudaPointerGetAttributes(&ga, gradient_wave_batches_compress) == cudaSuccess &&
+                        wa.type == cudaMemoryTypeDevice && ga.type == cudaMemoryTypeDevice &&
+                        wa.device == S.device && ga.device == S.device;
+  cudaGetLastError();
+  if (dev_wave) {
+    S.wave = wave_batches_compress;
+    S.gwave = gradient_wave_batches_compress;
+    S.borrowed_wave = true;
+  } else {
+    alloc((void **)&S.wave, sizeof(double) * wl);
+    alloc((void **)&S.gwave, sizeof(double) * 3 * wl);
+  }
   alloc((void **)&S.P1, sizeof(double) * (size_t)S.n_basis * S.n_basis * T);
   alloc((void **)&S.bias, sizeof(double) * nbias);
   alloc((void **)&S.gbias, sizeof(double) * 3 * nbias);
   alloc((void **)&S.out_rho, sizeof(double) * (size_t)S.n_full_points * T);
   alloc((void **)&S.out_grad, sizeof(double) * 3 * nbias);
-  if (t_status == FRPA_OK &&
+  if (t_status == FRPA_OK && !dev_wave &&
       (cudaMemcpy(S.wave, wave_batches_compress, sizeof(double) * wl, cudaMemcpyHostToDevice) != cudaSuccess ||
        cudaMemcpy(S.gwave, gradient_wave_batches_compress, sizeof(double) * 3 * wl, cudaMemcpyHostToDevice) !=
            cudaSuccess))

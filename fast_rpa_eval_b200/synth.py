@@ -577,3 +577,53 @@ def config3(l_max: int = 6, seed: int = 4, n_atoms: int = 500, n_points: int = 2
     args = dict(outer_radius=None, near_radius=2.0, spline_scale=1e-2)
     args.update(kw)
     return make_sumup_problem(n_atoms=n_atoms, n_points=n_points, l_pot_max=l_max, seed=seed, **args)
+
+
+def subset_batches(prob: Rho1Problem, n_batches: int, wave=None, gradient_wave=None) -> Rho1Problem:
+    """The first ``n_batches`` batches of ``prob`` as a standalone problem whose
+    points are renumbered 0..n-1 (the identity valid-to-full map).  ``wave`` /
+    ``gradient_wave`` default to prob's arrays cut to the subset's extent."""
+    nb = int(min(n_batches, prob.n_my_batches_work))
+    pre = prob.n_point_batches_prefix_sum[: nb + 1].astype(np.int32).copy()
+    off = prob.i_batch_2_wave_offset[: nb + 1].astype(np.int32).copy()
+    n_valid, wl = int(pre[-1]), int(off[-1])
+    w = (prob.wave if wave is None else wave)[:wl]
+    gw = (prob.gradient_wave if gradient_wave is None else gradient_wave)[: 3 * wl]
+    T = prob.T
+    return Rho1Problem(
+        T=T, j_atom_begin=prob.j_atom_begin, j_atom_end=prob.j_atom_end, j_coord=prob.j_coord, n_my_batches_work=nb,
+        n_full_points=max(1, n_valid), n_basis=prob.n_basis, n_atoms=prob.n_atoms,
+        n_max_compute_ham=prob.n_max_compute_ham, n_centers_basis_I=prob.n_centers_basis_I,
+        n_max_batch_size=prob.n_max_batch_size, batch_sizes=prob.batch_sizes[:nb].copy(),
+        n_point_batches=prob.n_point_batches[:nb].copy(), n_point_batches_prefix_sum=pre,
+        i_valid_point_2_i_full_points_map=np.arange(max(1, n_valid), dtype=np.int32),
+        n_compute_c_batches=prob.n_compute_c_batches[:nb].copy(),
+        i_basis_batches=np.asfortranarray(prob.i_basis_batches[:, :nb]),
+        atom_valid_n_compute_c_batches=np.asfortranarray(prob.atom_valid_n_compute_c_batches[:, :nb]),
+        i_batch_2_wave_offset=off, wave=np.ascontiguousarray(w), gradient_wave=np.ascontiguousarray(gw),
+        first_order_density_matrix=prob.first_order_density_matrix,
+        first_order_rho_bias_part2=np.asfortranarray(prob.first_order_rho_bias_part2[:, :nb, :]),
+        first_order_gradient_rho_bias=np.asfortranarray(prob.first_order_gradient_rho_bias[:, :, :nb, :]),
+        basis_atom=prob.basis_atom, partition_tab=np.ones(max(1, n_valid)), density_matrix=None,
+        atoms_xyz=prob.atoms_xyz, basis=prob.basis,
+        valid_points_xyz=None if prob.valid_points_xyz is None else prob.valid_points_xyz[:n_valid],
+    )
+
+
+def host_basis_values(prob: Rho1Problem, n_batches: int | None = None, pad_value: float = 0.0):
+    """Host (numpy) wave / gradient_wave for the first ``n_batches`` batches."""
+    nb = prob.n_my_batches_work if n_batches is None else int(n_batches)
+    wl = int(prob.i_batch_2_wave_offset[nb])
+    wave = np.full(wl, pad_value)
+    gwave = np.full(3 * wl, pad_value)
+    pre, off = prob.n_point_batches_prefix_sum, prob.i_batch_2_wave_offset
+    for b in range(nb):
+        nc, npb = int(prob.n_compute_c_batches[b]), int(prob.n_point_batches[b])
+        if nc == 0 or npb == 0:
+            continue
+        ncp = (nc + 3) // 4 * 4
+        ib = prob.i_basis_batches[:nc, b] - 1
+        phi, gphi = eval_basis(prob.basis, ib, prob.atoms_xyz, prob.valid_points_xyz[pre[b]:pre[b] + npb])
+        wave[off[b]:off[b] + ncp * npb].reshape(npb, ncp)[:, :nc] = phi.T
+        gwave[3 * off[b]:3 * off[b] + 3 * ncp * npb].reshape(npb, 3, ncp)[:, :, :nc] = np.transpose(gphi, (2, 1, 0))
+    return wave, gwave

@@ -147,7 +147,9 @@ void free_dfpt_device_info(void);
 /* Replaces init_dfpt_device_data (device_data.hpp:159-225, device_data.cu:10-361):
  * validates and uploads the constant arrays once, builds the rho1 work list
  * (the reference's valid-batch list and per-tile GEMM metadata,
- * device_data.cu:242-300) and the sum-up plan. */
+ * device_data.cu:242-300) and the sum-up plan.  Wave arrays that are already
+ * device memory of the session's GPU are used in place (not copied); the
+ * caller keeps them alive until free_dfpt_device_data. */
 void init_dfpt_device_data(
     int *n_my_batches_work, int *n_full_points, int *n_valid_points, int *n_basis, int *n_atoms,
     int *n_max_compute_ham, int *n_centers_basis_I, int *n_max_batch_size, int *l_pot_max, int *n_max_radial,
@@ -272,6 +274,14 @@ int frpa_sumup_device_flags(const frpa_sumup_plan *plan, int *flags);
 int frpa_synth_basis_values(const frpa_rho1_desc *desc, const double *points, int n_atoms, const double *atoms,
                             const int *basis_atom, const int *basis_l, const int *basis_m, const double *basis_alpha,
                             double pad_value, double *wave, double *gradient_wave, void *stream);
+
+/* Measured FP64 tensor-pipe throughput of the current device (independent
+ * m8n8k4 f64 MMAs on every SM), the ceiling the plain FP64 rho1 contraction
+ * is compared against.  Takes a few tens of milliseconds. */
+int frpa_probe_fp64_mma_tflops(double *tflops, void *stream);
+/* Same for the FP64 FMA pipe (independent DFMA chains), the ceiling of the
+ * sum-up kernels. */
+int frpa_probe_fp64_fma_tflops(double *tflops, void *stream);
 
 #ifdef __cplusplus
 }

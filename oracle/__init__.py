@@ -271,3 +271,118 @@ def rho_bias_part2(prob, density_matrix, T: int = 4, use_reference: bool = False
             A.d(prob.wave), A.d(prob.gradient_wave), out.ctypes.data_as(c_dbl_p), A.d(prob.partition_tab),
             A.d(density_matrix))
     return out.reshape((nmb, nb, T), order="F")
+
+
+# --------------------------------------------------------------------------
+# CPU baseline: the reference's rho1 over all host threads
+# --------------------------------------------------------------------------
+
+
+def _openblas_single_thread():
+    """The reference links a sequential BLAS (MKL sequential); pin the shared
+    OpenBLAS to one thread so batch-parallel threads do not oversubscribe."""
+    import glob
+
+    import numpy
+
+    libdir = os.path.realpath(os.path.join(os.path.dirname(numpy.__file__), "..", "numpy.libs"))
+    for path in glob.glob(os.path.join(libdir, "libscipy_openblas*")):
+        try:
+            ob = ctypes.CDLL(path)
+            for name in ("scipy_openblas_set_num_threads64_", "scipy_openblas_set_num_threads_64_"):
+                if hasattr(ob, name):
+                    getattr(ob, name)(c_int(1))
+                    return True
+        except OSError:
+            pass
+    return False
+
+
+def rho1_reference_threaded(prob, n_threads: int):
+    """Runs the reference's evaluate_first_order_rho_reduce_memory_c_v3_batches_atoms_
+    (oracle/_ref, T = 1) over prob's batches split into n_threads contiguous,
+    cost-balanced slices, one host thread per slice (the reference itself is
+    single-threaded).  Returns (rho, grad) assembled from the slices."""
+    import concurrent.futures as cf
+
+    assert prob.T == 1, "threaded baseline slices the batch axis; T = 1 only"
+    _openblas_single_thread()
+    lib = _load(os.path.join("_ref", "libref_t1.so"))
+    nb, nmb = prob.n_my_batches_work, prob.n_max_batch_size
+    cost = prob.n_compute_c_batches.astype(np.float64) ** 2 * prob.n_point_batches
+    cum = np.concatenate([[0.0], np.cumsum(cost)])
+    cuts = [0] + [int(np.searchsorted(cum, cum[-1] * k / n_threads)) for k in range(1, n_threads)] + [nb]
+    cuts = sorted(set(min(max(c, 0), nb) for c in cuts))
+    A = _Args()
+    arr = dict(
+        bs=_i(prob.batch_sizes)[0], npb=_i(prob.n_point_batches)[0], pre=_i(prob.n_point_batches_prefix_sum)[0],
+        map=_i(prob.i_valid_point_2_i_full_points_map)[0], ncb=_i(prob.n_compute_c_batches)[0],
+        ib=_i(prob.i_basis_batches)[0], avn=_i(prob.atom_valid_n_compute_c_batches)[0],
+        off=_i(prob.i_batch_2_wave_offset)[0], wave=_d(prob.wave)[0], gwave=_d(prob.gradient_wave)[0],
+        P1=_d(prob.first_order_density_matrix)[0], bias=_d(prob.first_order_rho_bias_part2)[0],
+        gbias=_d(prob.first_order_gradient_rho_bias)[0], ba=_i(prob.basis_atom)[0], pt=_d(prob.partition_tab)[0])
+    grad = np.zeros(3 * nmb * nb)
+    rhos = []
+
+    def ip(a, off=0):
+        return ctypes.cast(a.ctypes.data + 4 * off, c_int_p)
+
+    def dp(a, off=0):
+        return ctypes.cast(a.ctypes.data + 8 * off, c_dbl_p)
+
+    def run(s0, s1):
+        rho = np.zeros(prob.n_full_points)
+        scal = [ctypes.byref(c_int(int(v))) for v in (
+            s1 - s0, prob.j_atom_begin, prob.j_atom_end, prob.j_coord, prob.n_full_points, prob.n_basis,
+            prob.n_atoms, prob.n_max_compute_ham, prob.n_centers_basis_I, nmb)]
+        lib.evaluate_first_order_rho_reduce_memory_c_v3_batches_atoms_(
+            *scal, ip(arr["bs"], s0), ip(arr["npb"], s0), ip(arr["pre"], s0), ip(arr["map"]), ip(arr["ncb"], s0),
+            ip(arr["ib"], s0 * prob.n_centers_basis_I), ip(arr["avn"], s0 * (prob.n_atoms + 1)), ip(arr["off"], s0),
+            dp(arr["wave"]), dp(arr["gwave"]), dp(arr["P1"]), rho.ctypes.data_as(c_dbl_p), dp(arr["bias"], s0 * nmb),
+            dp(grad, 3 * nmb * s0), dp(arr["gbias"], 3 * nmb * s0), ip(arr["ba"]), dp(arr["pt"]), dp(arr["P1"]))
+        return rho
+
+    with cf.ThreadPoolExecutor(max_workers=max(1, len(cuts) - 1)) as ex:
+        rhos = list(ex.map(lambda ab: run(*ab), zip(cuts[:-1], cuts[1:])))
+    del A
+    rho = np.sum(rhos, axis=0) if rhos else np.zeros(prob.n_full_points)
+    return rho.reshape((prob.n_full_points, 1), order="F"), grad.reshape((3, nmb, nb, 1), order="F")
+
+
+def sumup_reference_threaded(prob, n_threads: int):
+    """The reference's sum-up (oracle/_ref) with the valid points split into
+    n_threads contiguous slices, one host thread each (outputs are disjoint
+    full points).  Returns the accumulated delta_v_hartree."""
+    import concurrent.futures as cf
+
+    T = prob.T
+    lib = _load(os.path.join("_ref", f"libref_t{T}.so"))
+    dv = np.array(prob.delta_v_hartree, dtype=np.float64).ravel(order="F").copy()
+    A = _Args()
+    ptrs = dict(
+        nr=A.i(prob.n_radial), sp=A.i(prob.species), spc=A.i(prob.species_center),
+        lh=A.i(prob.l_hartree_max_far_distance), xyz=A.d(prob.coord_points), mrs=A.d(prob.multipole_radius_sq),
+        opr=A.d(prob.outer_potential_radius), q=A.d(prob.multipole_moments), spl=A.d(prob.spline),
+        lhs=A.i(prob.l_hartree), ng=A.i(prob.n_grid), ncc=A.i(prob.n_cc_lm_ijk),
+        chp=A.i(prob.centers_hartree_potential), c2a=A.i(prob.center_to_atom), icc=A.i(prob.index_cc),
+        ijk=A.i(prob.index_ijk_max_cc), cc=A.d(prob.cc), cxyz=A.d(prob.coords_center), rgm=A.d(prob.r_grid_min),
+        linc=A.d(prob.log_r_grid_inc), scl=A.d(prob.scale_radial), pt=A.d(prob.partition_tab))
+    vmap = np.ascontiguousarray(prob.i_valid_point_2_i_full_points_map, dtype=np.int32)
+    n = prob.n_valid_points
+    cuts = [n * k // n_threads for k in range(n_threads + 1)]
+
+    def run(a, b):
+        scal = [ctypes.byref(c_int(int(v))) for v in (
+            prob.j_atom_begin, prob.j_atom_end, prob.n_full_points, prob.l_max_analytic_multipole,
+            prob.index_cc_dim_0, b - a, prob.l_pot_max, prob.n_max_radial, prob.n_hartree_grid, prob.n_centers,
+            prob.n_centers_hartree_potential, prob.n_atoms, prob.hartree_force_l_add, prob.n_species)]
+        p = ptrs
+        lib.sum_up_whole_potential_c_v3_atoms_full_points_j_atom_tile_(
+            *scal, p["nr"], p["sp"], p["spc"], p["lh"], ctypes.cast(vmap.ctypes.data + 4 * a, c_int_p), p["xyz"],
+            p["mrs"], p["opr"], p["q"], p["spl"], p["lhs"], p["ng"], p["ncc"], p["chp"], p["c2a"], p["icc"],
+            p["ijk"], p["cc"], p["cxyz"], p["rgm"], p["linc"], p["scl"], p["pt"], dv.ctypes.data_as(c_dbl_p))
+
+    with cf.ThreadPoolExecutor(max_workers=n_threads) as ex:
+        list(ex.map(lambda ab: run(*ab), [(cuts[k], cuts[k + 1]) for k in range(n_threads) if cuts[k + 1] > cuts[k]]))
+    del A
+    return dv.reshape((prob.n_full_points, T), order="F")
