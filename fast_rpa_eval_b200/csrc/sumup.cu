@@ -37,6 +37,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <mutex>
 #include <vector>
 
 #include "frpa_internal.cuh"
@@ -868,3 +869,122 @@ int sumup_adjoint_q(const SumupPlan *P, int n_active, const int *lhmfd, const do
 }
 
 }  // namespace frpa
+
+// ------------------------------------------------ allocation-free variant
+//
+// frpa_sumup_execute_noalloc: the sum-up for callers that cannot let a
+// library call cudaMalloc / cudaFree, such as a host code that hands the GPU
+// a fixed memory budget managed by its own pool, or one that keeps several
+// streams busy and cannot afford cudaFree's implicit device-wide
+// synchronisation.  The caller passes every input and the output as device
+// pointers; the only scratch this path needs (the packed multipole table and
+// the per-atom multipole coefficients) lives in the file-scope array below,
+// which every GPU that loads the library holds until the process exits.
+// It runs the reference-mirroring (generic) kernel.
+
+namespace frpa {
+
+constexpr size_t NOALLOC_SCRATCH_BYTES = 8u << 20;  // 8 MiB per device
+static __device__ __align__(256) unsigned char g_noalloc_scratch[NOALLOC_SCRATCH_BYTES];
+
+namespace {
+
+__global__ void noalloc_pack_table_kernel(int n_rows, int icc_dim0, const int *__restrict__ icc,
+                                          int *__restrict__ packed) {
+  for (int n = blockIdx.x * blockDim.x + threadIdx.x; n < n_rows; n += gridDim.x * blockDim.x)
+    packed[n] = icc[n + 2 * icc_dim0] | (icc[n + 3 * icc_dim0] << 8) | (icc[n + 4 * icc_dim0] << 16) |
+                (icc[n + 5 * icc_dim0] << 24);
+}
+
+std::mutex g_noalloc_mu;
+void *g_noalloc_addr[64] = {nullptr};
+
+// Device address of the scratch array for the current device, looked up once
+// per device (host code may not use the array's name as an address).
+int noalloc_scratch_address(int device, unsigned char **out) {
+  std::lock_guard<std::mutex> lk(g_noalloc_mu);
+  if (device < 0 || device >= 64) return fail(FRPA_ERR_UNSUPPORTED, "noalloc sum-up: device %d", device);
+  if (!g_noalloc_addr[device]) {
+    void *p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess)
+      return fail(FRPA_ERR_CUDA, "noalloc sum-up: cudaGetSymbolAddress failed: %s", cudaGetErrorString(e));
+    FRPA_TRY(sumup_upload_constants(device));
+    g_noalloc_addr[device] = p;
+  }
+  *out = static_cast<unsigned char *>(g_noalloc_addr[device]);
+  return FRPA_OK;
+}
+
+}  // namespace
+}  // namespace frpa
+
+extern "C" int frpa_sumup_execute_noalloc(
+    int atom_tile_size, int j_atom_begin, int j_atom_end, int n_full_points, int l_max_analytic_multipole,
+    int index_cc_dim_0, int n_valid_points, int l_pot_max, int n_hartree_grid, int n_centers,
+    int n_centers_hartree_potential, int n_atoms, int hartree_force_l_add, int n_species, const int *species,
+    const int *species_center, const int *l_hartree_max_far_distance, const int *i_valid_point_2_i_full_points_map,
+    const double *coord_points, const double *multipole_radius_sq, const double *outer_potential_radius,
+    const double *multipole_moments, const double *spline, const int *l_hartree, const int *n_grid,
+    const int *n_cc_lm_ijk, const int *centers_hartree_potential, const int *center_to_atom, const int *index_cc,
+    const int *index_ijk_max_cc, const double *cc, const double *coords_center, const double *r_grid_min,
+    const double *log_r_grid_inc, double *delta_v_hartree, void *stream_) {
+  using namespace frpa;
+  clear_error();
+  const int T = atom_tile_size, L = l_pot_max, n_active = j_atom_end - j_atom_begin + 1;
+  FRPA_CHECK_ARG(T >= 1 && T <= FRPA_MAX_ATOM_TILE, "noalloc sum-up: atom tile size %d out of range", T);
+  FRPA_CHECK_ARG(L >= 0 && L <= SU_LMAX, "noalloc sum-up: l_pot_max %d unsupported (0..%d)", L, SU_LMAX);
+  FRPA_CHECK_ARG(l_max_analytic_multipole >= L && index_cc_dim_0 > 0, "noalloc sum-up: bad multipole table sizes");
+  FRPA_CHECK_ARG(hartree_force_l_add >= 0 && L + hartree_force_l_add <= 2 * SU_LMAX + 3,
+                 "noalloc sum-up: hartree_force_l_add %d out of range", hartree_force_l_add);
+  FRPA_CHECK_ARG(n_active <= T, "noalloc sum-up: j_atom_end - j_atom_begin + 1 = %d > ATOM_TILE_SIZE %d", n_active, T);
+  FRPA_CHECK_ARG(n_full_points >= 0 && n_valid_points >= 0 && n_valid_points <= n_full_points && n_atoms > 0 &&
+                     n_centers > 0 && n_centers_hartree_potential >= 0 &&
+                     n_centers_hartree_potential <= n_centers && n_species > 0 && n_hartree_grid >= 2,
+                 "noalloc sum-up: bad sizes");
+  FRPA_CHECK_ARG(species && species_center && l_hartree_max_far_distance && i_valid_point_2_i_full_points_map &&
+                     coord_points && multipole_radius_sq && outer_potential_radius && multipole_moments && spline &&
+                     l_hartree && n_grid && n_cc_lm_ijk && centers_hartree_potential && center_to_atom && index_cc &&
+                     index_ijk_max_cc && cc && coords_center && r_grid_min && log_r_grid_inc && delta_v_hartree,
+                 "noalloc sum-up: null device pointer");
+  // scratch layout: [error flag | packed table rows | multipole coefficients
+  // (index_cc_dim_0, n_atoms, T)]; the coefficient block is sized by
+  // index_cc_dim_0, an upper bound of n_cc_lm_ijk[l_pot_max] known on the host.
+  const size_t flag_bytes = 256;
+  const size_t table_bytes = ((size_t)index_cc_dim_0 * sizeof(int) + 255) / 256 * 256;
+  const size_t mc_bytes = sizeof(double) * (size_t)index_cc_dim_0 * n_atoms * T;
+  const size_t need = flag_bytes + table_bytes + mc_bytes;
+  FRPA_CHECK_ARG(need <= NOALLOC_SCRATCH_BYTES,
+                 "noalloc sum-up: needs %zu bytes of scratch (index_cc_dim_0 %d x n_atoms %d x tile %d), more than "
+                 "the %zu bytes this entry point has; use frpa_sumup_plan_create / frpa_sumup_execute",
+                 need, index_cc_dim_0, n_atoms, T, (size_t)NOALLOC_SCRATCH_BYTES);
+  int device = 0;
+  FRPA_CUDA_TRY(cudaGetDevice(&device));
+  unsigned char *base = nullptr;
+  FRPA_TRY(noalloc_scratch_address(device, &base));
+  if (n_active <= 0 || n_valid_points == 0 || n_centers_hartree_potential == 0) return FRPA_OK;
+  cudaStream_t stream = (cudaStream_t)stream_;
+  int *err = reinterpret_cast<int *>(base);
+  int *packed = reinterpret_cast<int *>(base + flag_bytes);
+  double *mc = reinterpret_cast<double *>(base + flag_bytes + table_bytes);
+  const int L2 = (L + 1) * (L + 1);
+  // every scratch word read below is written first in this call, so nothing
+  // left by an earlier call is used; the flag is cleared explicitly
+  FRPA_CUDA_TRY(cudaMemsetAsync(err, 0, sizeof(int), stream));
+  noalloc_pack_table_kernel<<<(index_cc_dim_0 + 255) / 256, 256, 0, stream>>>(index_cc_dim_0, index_cc_dim_0,
+                                                                               index_cc, packed);
+  FRPA_LAUNCH_CHECK();
+  sumup_multipole_c_kernel<<<dim3(n_atoms, n_active), 128, 0, stream>>>(
+      n_atoms, L, L2, index_cc_dim_0, index_cc_dim_0, l_max_analytic_multipole, index_cc, n_cc_lm_ijk, cc,
+      l_hartree_max_far_distance, multipole_moments, mc, err);
+  FRPA_LAUNCH_CHECK();
+  const int grid = (n_valid_points + SU_THREADS - 1) / SU_THREADS;
+  sumup_generic_kernel<<<grid, SU_THREADS, 0, stream>>>(
+      n_valid_points, n_full_points, i_valid_point_2_i_full_points_map, coord_points, n_active,
+      n_centers_hartree_potential, n_atoms, L, L2, n_hartree_grid, hartree_force_l_add, centers_hartree_potential,
+      center_to_atom, species, species_center, l_hartree, n_grid, r_grid_min, log_r_grid_inc, coords_center,
+      multipole_radius_sq, outer_potential_radius, n_cc_lm_ijk, packed, index_ijk_max_cc, index_cc_dim_0, mc, spline,
+      delta_v_hartree, nullptr);
+  FRPA_LAUNCH_CHECK();
+  return FRPA_OK;
+}

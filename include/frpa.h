@@ -258,6 +258,32 @@ int frpa_sumup_adjoint_q(const frpa_sumup_plan *plan, int n_active, const int *l
                          const double *multipole_radius_sq, const double *outer_potential_radius,
                          const double *multipole_moments, const double *g, double *dQ, void *stream);
 
+/* The sum-up without any device allocation, for callers that cannot let a
+ * library call cudaMalloc or cudaFree: host codes that give the GPU a fixed
+ * memory budget run by their own pool, or that keep several streams busy and
+ * cannot take cudaFree's device-wide synchronisation.  No counterpart in the
+ * reference.  Arguments as sum_up_..._cu_host_ with ALL arrays as device
+ * pointers, the tile size explicit and a stream; accumulates into
+ * delta_v_hartree with the reference-mirroring kernel.  Its scratch is one
+ * 8 MiB array inside the library per GPU, held until the process exits, which
+ * limits 256 + 4 index_cc_dim_0 (rounded to 256) + 8 index_cc_dim_0 n_atoms T
+ * bytes to 8 MiB; larger inputs are rejected with FRPA_ERR_INVALID.  Calls
+ * share that array, so calls that overlap on the GPU (other streams, other
+ * threads) race and must be serialised by the caller.  The first call on a
+ * device looks the array up (and loads the library's constants); make it
+ * before any stream capture.  Device arrays are not range-checked: pass data
+ * that frpa_sumup_plan_create would accept. */
+int frpa_sumup_execute_noalloc(
+    int atom_tile_size, int j_atom_begin, int j_atom_end, int n_full_points, int l_max_analytic_multipole,
+    int index_cc_dim_0, int n_valid_points, int l_pot_max, int n_hartree_grid, int n_centers,
+    int n_centers_hartree_potential, int n_atoms, int hartree_force_l_add, int n_species, const int *species,
+    const int *species_center, const int *l_hartree_max_far_distance, const int *i_valid_point_2_i_full_points_map,
+    const double *coord_points, const double *multipole_radius_sq, const double *outer_potential_radius,
+    const double *multipole_moments, const double *spline, const int *l_hartree, const int *n_grid,
+    const int *n_cc_lm_ijk, const int *centers_hartree_potential, const int *center_to_atom, const int *index_cc,
+    const int *index_ijk_max_cc, const double *cc, const double *coords_center, const double *r_grid_min,
+    const double *log_r_grid_inc, double *delta_v_hartree, void *stream);
+
 /* Reads and clears the device-side input flags of the last executions
  * (bit 0: an l_hartree_max_far_distance entry outside 0..l_pot_max, clamped). */
 int frpa_sumup_device_flags(const frpa_sumup_plan *plan, int *flags);
