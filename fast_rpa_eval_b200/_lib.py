@@ -190,6 +190,11 @@ class Rho1Plan:
         check(lib().frpa_rho1_execute(self.handle, c_int(mode), c_int(n_active), _ptr(wave), _ptr(gwave), _ptr(P1),
                                       _ptr(bias), _ptr(gbias), _ptr(rho), _ptr(grad), _stream(stream)))
 
+    def device_flags(self) -> int:
+        f = c_int(0)
+        check(lib().frpa_rho1_device_flags(self.handle, ctypes.byref(f)))
+        return f.value
+
     def adjoint_p1(self, n_active, wave, gwave, g_rho, g_grad, dP1, stream=None):
         check(lib().frpa_rho1_adjoint_p1(self.handle, c_int(n_active), _ptr(wave), _ptr(gwave), _ptr(g_rho),
                                          _ptr(g_grad), _ptr(dP1), _stream(stream)))

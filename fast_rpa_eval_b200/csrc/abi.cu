@@ -56,9 +56,6 @@ int sumup_read_error_flags(const SumupPlan *P, int *flags);
 int synth_basis_values(const frpa_rho1_desc *D, const double *points, int n_atoms, const double *atoms,
                        const int *basis_atom, const int *basis_l, const int *basis_m, const double *basis_alpha,
                        double pad, double *wave, double *gwave, cudaStream_t stream);
-int rho1_split_launch(const Rho1Plan &plan, int n_active, const double *wave, const double *gwave,
-                      const double *P1, const double *bias, const double *gbias, double *rho, double *grad,
-                      cudaStream_t stream);
 
 // ------------------------------------------------------------- rho1 plan
 
@@ -69,6 +66,9 @@ static void rho1_plan_free(Rho1Plan *P) {
   cudaFree(P->d_map);
   cudaFree(P->d_counter);
   cudaFree(P->d_adj_items);
+  cudaFree(P->d_items_split);
+  cudaFree(P->d_rowmax);
+  cudaFree(P->d_err);
   delete P;
 }
 
@@ -161,6 +161,18 @@ static int rho1_plan_build(Rho1Plan **out, const frpa_rho1_desc *D) {
       st = fail(FRPA_ERR_CUDA, "rho1: plan upload failed");
   };
   up((void **)&P->d_items, items.data(), sizeof(Rho1WorkItem) * items.size());
+  {
+    std::vector<Rho1WorkItem> split;
+    std::vector<int> npb(nb);
+    for (int b = 0; b < nb; ++b) npb[b] = D->n_point_batches[b];
+    rho1_split_build_items(items, npb.data(), nb, &split);
+    P->n_items_split = (int)split.size();
+    up((void **)&P->d_items_split, split.data(), sizeof(Rho1WorkItem) * split.size());
+    std::vector<double> zeros((size_t)D->n_basis * T, 0.0);
+    up((void **)&P->d_rowmax, zeros.data(), sizeof(double) * zeros.size());
+    const int z = 0;
+    up((void **)&P->d_err, &z, sizeof(int));
+  }
   up((void **)&P->d_ib, ibc.data(), sizeof(int) * ibc.size());
   up((void **)&P->d_map, D->i_valid_point_2_i_full_points_map, sizeof(int) * (size_t)map_len);
   const int zero = 0;
@@ -420,6 +432,13 @@ int frpa_rho1_execute(const frpa_rho1_plan *plan, int mode, int n_active, const 
                       double *rho, double *grad, void *stream) {
   if (!plan) return fail(FRPA_ERR_INVALID, "rho1: null plan");
   return rho1_run(*plan->p, mode, n_active, wave, gradient_wave, P1, bias, gbias, rho, grad, (cudaStream_t)stream);
+}
+
+int frpa_rho1_device_flags(const frpa_rho1_plan *plan, int *flags) {
+  if (!plan || !flags) return fail(FRPA_ERR_INVALID, "rho1: null argument");
+  FRPA_CUDA_TRY(cudaMemcpy(flags, plan->p->d_err, sizeof(int), cudaMemcpyDeviceToHost));
+  FRPA_CUDA_TRY(cudaMemset(plan->p->d_err, 0, sizeof(int)));
+  return FRPA_OK;
 }
 
 int frpa_rho1_adjoint_p1(const frpa_rho1_plan *plan, int n_active, const double *wave, const double *gradient_wave,

@@ -119,12 +119,22 @@ struct Rho1Plan {
   // adjoint work list (batch, i tile, j tile, t), built with the plan
   void *d_adj_items = nullptr;
   int n_adj_items = 0;
+  // split-BF16 path: <= 128-point tiles, per-row P1 scales, device error flags
+  Rho1WorkItem *d_items_split = nullptr;
+  int n_items_split = 0;
+  double *d_rowmax = nullptr;
+  int *d_err = nullptr;
 };
 
 int rho1_fp64_launch(const Rho1Plan &plan, int n_active, const double *wave, const double *gwave,
                      const double *P1, const double *bias, const double *gbias, double *rho, double *grad,
                      cudaStream_t stream);
 int rho1_fp64_grid(int device);
+int rho1_split_launch(const Rho1Plan &plan, int n_active, const double *wave, const double *gwave,
+                      const double *P1, const double *bias, const double *gbias, double *rho, double *grad,
+                      cudaStream_t stream);
+void rho1_split_build_items(const std::vector<Rho1WorkItem> &fp64_items, const int *np_b, int n_batches,
+                            std::vector<Rho1WorkItem> *out);
 
 int rho1_adjoint_launch_items(const Rho1Plan &plan, const void *d_items, int n_items, int n_active,
                               const double *wave, const double *gwave, const double *g_rho, const double *g_grad,

@@ -1,14 +1,596 @@
-// Split-precision rho1 contraction (placeholder until the tcgen05 kernel lands).
+// Split-precision rho1: the contraction work1 = P1c * phi on the 5th-generation
+// tensor cores (tcgen05, BF16 in, FP32 accumulate in TMEM) at FP64-grade
+// accuracy, with the per-point dot products in FP64.
+//
+// Same semantics as the plain FP64 path (rho1_fp64.cu,
+// fast_rap_src_dfpt_gpu_eval/evaluate_first_order_rho.cpp:116-209).
+//
+// Numerics.  Every FP64 operand element x of a row with power-of-two scale
+// 2^e >= max|x| is written as y = x 2^-e in [-1, 1] and split into five BF16
+// slices, y ~ 2^-7 (S0 + S1 + S2 + S3 + S4), S_s = a_s 2^(-8 s), with integer
+// digits |a_0| <= 128 (7 bits) and |a_s| <= 128 (8 bits, round to nearest) --
+// 39 bits in all, each slice exact in BF16.  The product of two split rows is
+// summed as 15 slice products (s + t <= 4) in four FP32 TMEM accumulators, one
+// per slice level s + t:
+//   acc0 = S0 S0,  acc1 = S0 S1 + S1 S0,  acc2 = S0 S2 + S1 S1 + S2 S0   (exact)
+//   acc3 = the levels 3 and 4                                           (rounded)
+// and recombined in FP64: work1(i, p) = 2^(eA_p + eB_i - 14) (acc0 + acc1 + acc2 + acc3).
+// The three exact levels are integer sums (in units of their level) of at most
+// 2^14, 2^15 and 3 2^14 per K step, so they cannot leave the FP32 integer range
+// for K <= 1024, 512 and 341; past those bounds they stay exact unless the sums
+// of residual digits (which behave like random signs) grow ~100x beyond their
+// typical size.  Only levels 3-4, 2^-24 below the result, see the tensor core's
+// FP32 truncation.  The benchmark recipes give normwise errors of ~2e-11.
+//
+// Data flow (one persistent CTA per SM, warp-specialised, 416 threads):
+//   * a work item is one batch's tile of <= 128 points; the MMA computes
+//     D[p, i] = sum_k Phi^T[p, k] P1c^T[k, i] (M = 128 points, N = 128 rows i,
+//     K = 16 per instruction), so each TMEM lane is one grid point and the
+//     epilogue's per-point sums need no cross-thread reduction;
+//   * 8 producer warps read phi (FP64) and gather P1c (FP64), scale, split and
+//     store the 10 slice tiles of a 32-wide K chunk in shared memory
+//     (canonical K-major layout, no swizzle) -- a two-stage ring;
+//   * 1 warp owns TMEM (512 columns = 4 accumulators x 128) and issues the
+//     15 x 2 tcgen05.mma per stage, committing to mbarriers;
+//   * 4 epilogue warps read the accumulators (tcgen05.ld), recombine in FP64
+//     and contract with phi and grad phi (FP64, global memory).
+// Every mbarrier wait is bounded in time; on a timeout the kernel records an
+// error flag, lets in-flight MMAs finish (bounded), frees TMEM and returns.
+#include <cuda_bf16.h>
+
+#include <algorithm>
+#include <vector>
+
 #include "frpa_internal.cuh"
 
 namespace frpa {
+namespace {
+
+constexpr int SP_M = 128;         // points per work item (TMEM lanes)
+constexpr int SP_N = 128;         // rows i per N tile (accumulator columns)
+constexpr int SP_KC = 32;         // K per pipeline stage
+constexpr int SP_STAGES = 2;
+constexpr int SP_SLICES = 5;
+constexpr int SP_EPI_WARPS = 4;   // warps 0..3: epilogue (TMEM lanes 0..127)
+constexpr int SP_MMA_WARP = 4;    // warp 4: TMEM owner and MMA issuer
+constexpr int SP_PROD_WARPS = 8;  // warps 5..12: producers
+constexpr int SP_PROD0 = SP_MMA_WARP + 1;
+constexpr int SP_THREADS = 32 * (SP_EPI_WARPS + 1 + SP_PROD_WARPS);
+constexpr int SP_PROD_THREADS = 32 * SP_PROD_WARPS;
+constexpr int SP_MAX_K = 1024;    // exactness bound of the FP32 levels 0 and 1
+constexpr int SP_TILE_ELEMS = SP_M * SP_KC;           // one slice tile (bf16 elements)
+constexpr uint32_t SP_LBO = 128;                      // bytes between K-adjacent core matrices
+constexpr uint32_t SP_SBO = (SP_KC / 8) * 128;        // bytes between 8-row groups
+constexpr unsigned long long SP_WAIT_NS = 2000000000ull;  // 2 s per wait
+
+static_assert(SP_M == 128 && SP_N == 128, "instruction shape");
+
+struct SplitSmem {
+  __nv_bfloat16 A[SP_STAGES][SP_SLICES][SP_TILE_ELEMS];
+  __nv_bfloat16 B[SP_STAGES][SP_SLICES][SP_TILE_ELEMS];
+  double scaleA[2][SP_M];  // 2^(eA - 7) per point, by item parity
+  double invA[2][SP_M];    // 2^-eA
+  double scaleB[2][SP_N];  // 2^(eB - 7) per row i, by tile parity
+  double invB[2][SP_N];
+  unsigned long long full[SP_STAGES];
+  unsigned long long empty[SP_STAGES];
+  unsigned long long acc_full;
+  unsigned long long acc_empty;
+  unsigned long long drain;
+  unsigned long long sa_full[2];  // per-point scales of an item published (by item parity)
+  unsigned long long sb_full[2];  // per-row scales of a tile published (by tile parity)
+  uint32_t tmem_base;
+  int abort_flag;
+};
+
+// ---------------------------------------------------------------- PTX glue
+
+__device__ __forceinline__ uint32_t smem_u32(const void *p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ unsigned long long global_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+__device__ __forceinline__ void mbar_init(unsigned long long *bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count));
+}
+
+__device__ __forceinline__ void mbar_arrive(unsigned long long *bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(unsigned long long *bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+
+// Bounded wait: false (and the error flag set) if the phase does not
+// complete within SP_WAIT_NS or another role has already given up.
+__device__ __forceinline__ bool mbar_wait(unsigned long long *bar, uint32_t parity, volatile int *abort_flag,
+                                          int *err) {
+  if (mbar_try_wait(bar, parity)) return true;
+  const unsigned long long t0 = global_ns();
+  for (;;) {
+    if (mbar_try_wait(bar, parity)) return true;
+    if (*abort_flag) return false;
+    if (global_ns() - t0 > SP_WAIT_NS) {
+      *abort_flag = 1;
+      atomicOr(err, 2);
+      return false;
+    }
+  }
+}
+
+__device__ __forceinline__ void fence_proxy_async_smem() {
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+__device__ __forceinline__ void tc_fence_before() {
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+}
+__device__ __forceinline__ void tc_fence_after() {
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+}
+
+// Shared-memory matrix descriptor: K-major, no swizzle, version 1 (sm_100).
+__device__ __forceinline__ uint64_t smem_desc(uint32_t addr) {
+  uint64_t d = 0;
+  d |= (uint64_t)((addr & 0x3FFFF) >> 4);
+  d |= (uint64_t)(SP_LBO >> 4) << 16;
+  d |= (uint64_t)(SP_SBO >> 4) << 32;
+  d |= (uint64_t)1 << 46;  // version
+  return d;                // base offset 0, lbo mode 0, layout type 0 (no swizzle)
+}
+
+// Instruction descriptor: kind::f16, D = F32, A = B = BF16, both K-major,
+// N = 128, M = 128.
+constexpr uint32_t SP_IDESC = (1u << 4)                       // D format F32
+                              | (1u << 7)                     // A format BF16
+                              | (1u << 10)                    // B format BF16
+                              | ((uint32_t)(SP_N >> 3) << 17)  // N
+                              | ((uint32_t)(SP_M >> 4) << 24); // M
+
+__device__ __forceinline__ void umma_bf16(uint32_t d_tmem, uint64_t a_desc, uint64_t b_desc, uint32_t accumulate) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}"
+      ::"r"(d_tmem), "l"(a_desc), "l"(b_desc), "r"(SP_IDESC), "r"(accumulate));
+}
+
+__device__ __forceinline__ void umma_commit(unsigned long long *bar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
+               : "memory");
+}
+
+__device__ __forceinline__ void tmem_ld32(uint32_t taddr, float (&v)[32]) {
+  uint32_t r[32];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x32.b32 "
+      "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+      "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+        "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]),
+        "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]),
+        "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+      : "r"(taddr));
+#pragma unroll
+  for (int j = 0; j < 32; ++j) v[j] = __uint_as_float(r[j]);
+}
+
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16]) {
+  uint32_t r[16];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 "
+      "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+        "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+      : "r"(taddr));
+#pragma unroll
+  for (int j = 0; j < 16; ++j) v[j] = __uint_as_float(r[j]);
+}
+
+__device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
+
+// Byte offset of element (row r, k) in a K-major no-swizzle tile of SP_KC columns.
+__device__ __forceinline__ int tile_off(int r, int k) {
+  return (r >> 3) * SP_SBO + (k >> 3) * SP_LBO + (r & 7) * 16 + (k & 7) * 2;
+}
+
+// Five slices of 8 consecutive values (already scaled to [-1, 1]) written as
+// 16-byte rows into the slice tiles at byte offset `off`.
+__device__ __forceinline__ void split8_store(const double (&y)[8], __nv_bfloat16 (*tiles)[SP_TILE_ELEMS],
+                                             int off) {
+  double r[8];
+#pragma unroll
+  for (int j = 0; j < 8; ++j) r[j] = y[j] * 128.0;
+#pragma unroll
+  for (int s = 0; s < SP_SLICES; ++s) {
+    const float scale = (s == 0) ? 1.0f : __int_as_float((127 - 8 * s) << 23);  // 2^(-8 s)
+    uint32_t packed[4];
+#pragma unroll
+    for (int j = 0; j < 8; j += 2) {
+      const double a0 = rint(r[j]), a1 = rint(r[j + 1]);
+      r[j] = (r[j] - a0) * 256.0;
+      r[j + 1] = (r[j + 1] - a1) * 256.0;
+      const __nv_bfloat162 h = __floats2bfloat162_rn((float)a0 * scale, (float)a1 * scale);
+      packed[j / 2] = *reinterpret_cast<const uint32_t *>(&h);
+    }
+    *reinterpret_cast<uint4 *>(reinterpret_cast<char *>(tiles[s]) + off) =
+        make_uint4(packed[0], packed[1], packed[2], packed[3]);
+  }
+}
+
+// 2^e >= |m| with e from frexp (e = 0 for m = 0); returns {2^(e-7), 2^-e}.
+__device__ __forceinline__ void pow2_scale(double m, double *scale, double *inv) {
+  int e = 0;
+  if (m > 0.0) frexp(m, &e);
+  *scale = ldexp(1.0, e - 7);
+  *inv = ldexp(1.0, -e);
+}
+
+struct SplitParams {
+  const Rho1WorkItem *items;
+  int n_items;
+  const int *ib_all;
+  const int *map;
+  int T, n_active, n_basis, n_full_points, n_max_batch_size, n_batches;
+  const double *wave, *gwave, *P1, *bias, *gbias;
+  const double *rowmax;  // (n_basis, T): max_c |P1(r, c, t)|
+  double *rho, *grad;
+  int *err;
+};
+
+// Producer thread mapping: segment q in [0, 512) of a 128 x 32 tile is
+// (row, kseg) = ((q & 7) + 8 (q >> 5), (q >> 3) & 3): a quarter warp stores
+// eight rows' 16-byte chunks of one core-matrix column (conflict-free), and
+// the four lanes sharing a row are lanes l, l^8, l^16, l^24 of one warp.
+__device__ __forceinline__ void seg_of(int q, int *row, int *kseg) {
+  *row = (q & 7) + 8 * (q >> 5);
+  *kseg = (q >> 3) & 3;
+}
+
+__device__ void producer_role(const SplitParams &P, SplitSmem &S, int ptid, int lane) {
+  int *err = P.err;
+  volatile int *abort_flag = &S.abort_flag;
+  const long long nb2 = (long long)P.n_basis * P.n_basis;
+  uint32_t fill = 0, tile_ctr = 0, item_ctr = 0;
+  int rows[2], ksegs[2];
+  seg_of(ptid, &rows[0], &ksegs[0]);
+  seg_of(ptid + SP_PROD_THREADS, &rows[1], &ksegs[1]);
+  for (int it = blockIdx.x; it < P.n_items; it += gridDim.x, ++item_ctr) {
+    const Rho1WorkItem W = P.items[it];
+    const int nc = W.nc, pn = W.pn, ncp = (nc + 3) & ~3;
+    const double *phi = P.wave + W.wave_off + (long long)W.p0 * ncp;
+    const int *ib = P.ib_all + W.ib_off;
+    const int ip = item_ctr & 1;
+    // per-point scales: the four lanes sharing a row split its column
+    double invA[2];
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      const int r = rows[h];
+      double m = 0.0;
+      if (r < pn)
+        for (int k = ksegs[h]; k < nc; k += 4) m = fmax(m, fabs(phi[k + (long long)r * ncp]));
+      m = fmax(m, __shfl_xor_sync(0xffffffffu, m, 8));
+      m = fmax(m, __shfl_xor_sync(0xffffffffu, m, 16));
+      double sc;
+      pow2_scale(m, &sc, &invA[h]);
+      if (ksegs[h] == 0) S.scaleA[ip][r] = sc;
+    }
+    if (ksegs[0] == 0) mbar_arrive(&S.sa_full[ip]);
+    const int n_nt = (nc + SP_N - 1) / SP_N, n_kc = (nc + SP_KC - 1) / SP_KC;
+    for (int t = 0; t < P.T; ++t) {
+      const double *P1t = P.P1 + t * nb2;
+      for (int jn = 0; jn < n_nt; ++jn, ++tile_ctr) {
+        const int n0 = jn * SP_N, tp = tile_ctr & 1;
+        double invB[2];
+        int ibrow[2];
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+          const int i = n0 + rows[h];
+          ibrow[h] = i < nc ? ib[i] - 1 : 0;
+          const double m = i < nc ? P.rowmax[ibrow[h] + (long long)P.n_basis * t] : 0.0;
+          double sc;
+          pow2_scale(m, &sc, &invB[h]);
+          if (ksegs[h] == 0) S.scaleB[tp][rows[h]] = sc;
+        }
+        if (ksegs[0] == 0) mbar_arrive(&S.sb_full[tp]);
+        for (int kc = 0; kc < n_kc; ++kc, ++fill) {
+          const int stage = fill & 1;
+          const uint32_t use = fill >> 1;
+          if (!mbar_wait(&S.empty[stage], (use & 1) ^ 1, abort_flag, err)) return;
+          const int k0 = kc * SP_KC;
+#pragma unroll
+          for (int h = 0; h < 2; ++h) {
+            const int r = rows[h], k = k0 + 8 * ksegs[h];
+            double y[8];
+            // A = Phi^T: row = point r, columns k..k+7
+#pragma unroll
+            for (int j = 0; j < 8; ++j)
+              y[j] = (r < pn && k + j < nc) ? phi[k + j + (long long)r * ncp] * invA[h] : 0.0;
+            split8_store(y, S.A[stage], tile_off(r, 8 * ksegs[h]));
+            // B = P1c (K-major): row i = n0 + r, columns k..k+7
+            const bool rok = n0 + r < nc;
+#pragma unroll
+            for (int j = 0; j < 8; ++j)
+              y[j] = (rok && k + j < nc) ? P1t[ibrow[h] + (long long)(ib[k + j] - 1) * P.n_basis] * invB[h] : 0.0;
+            split8_store(y, S.B[stage], tile_off(r, 8 * ksegs[h]));
+          }
+          fence_proxy_async_smem();
+          __syncwarp();
+          if (lane == 0) mbar_arrive(&S.full[stage]);
+        }
+      }
+    }
+  }
+}
+
+__device__ void mma_role(const SplitParams &P, SplitSmem &S, uint32_t tmem) {
+  int *err = P.err;
+  volatile int *abort_flag = &S.abort_flag;
+  uint32_t fill = 0, tile_ctr = 0;
+  bool issued = false;
+  for (int it = blockIdx.x; it < P.n_items && !*abort_flag; it += gridDim.x) {
+    const int nc = P.items[it].nc;
+    const int n_nt = (nc + SP_N - 1) / SP_N, n_kc = (nc + SP_KC - 1) / SP_KC;
+    for (int t = 0; t < P.T; ++t)
+      for (int jn = 0; jn < n_nt; ++jn, ++tile_ctr) {
+        if (!mbar_wait(&S.acc_empty, (tile_ctr & 1) ^ 1, abort_flag, err)) goto done;
+        tc_fence_after();
+        for (int kc = 0; kc < n_kc; ++kc, ++fill) {
+          const int stage = fill & 1;
+          if (!mbar_wait(&S.full[stage], (fill >> 1) & 1, abort_flag, err)) goto done;
+          tc_fence_after();
+#pragma unroll
+          for (int ks = 0; ks < SP_KC / 16; ++ks) {
+            uint64_t a[SP_SLICES], b[SP_SLICES];
+#pragma unroll
+            for (int s = 0; s < SP_SLICES; ++s) {
+              a[s] = smem_desc(smem_u32(S.A[stage][s]) + ks * 2 * SP_LBO);
+              b[s] = smem_desc(smem_u32(S.B[stage][s]) + ks * 2 * SP_LBO);
+            }
+            const uint32_t acc = (kc > 0 || ks > 0) ? 1u : 0u;
+            // accumulator q holds slice level s + u = q (q < 3, exact) and the
+            // levels 3 and 4 (q = 3, rounded)
+            uint32_t first[4] = {acc, acc, acc, acc};
+#pragma unroll
+            for (int s = 0; s < SP_SLICES; ++s)
+#pragma unroll
+              for (int u = 0; u < SP_SLICES; ++u)
+                if (s + u <= 4) {
+                  const int q = s + u < 3 ? s + u : 3;
+                  umma_bf16(tmem + q * SP_N, a[s], b[u], first[q]);
+                  first[q] = 1u;
+                }
+          }
+          umma_commit(&S.empty[stage]);
+          issued = true;
+        }
+        umma_commit(&S.acc_full);
+      }
+  }
+done:
+  if (issued) {
+    // every MMA issued by this thread has completed once this commit arrives
+    umma_commit(&S.drain);
+    const unsigned long long t0 = global_ns();
+    while (!mbar_try_wait(&S.drain, 0)) {
+      if (global_ns() - t0 > SP_WAIT_NS) {
+        atomicOr(err, 4);
+        break;
+      }
+    }
+  }
+}
+
+__device__ void epilogue_role(const SplitParams &P, SplitSmem &S, uint32_t tmem, int warp, int lane) {
+  int *err = P.err;
+  volatile int *abort_flag = &S.abort_flag;
+  const int p = warp * 32 + lane;  // TMEM lane = point within the tile
+  const uint32_t lane_base = tmem + ((uint32_t)(warp * 32) << 16);
+  uint32_t tile_ctr = 0, item_ctr = 0;
+  for (int it = blockIdx.x; it < P.n_items; it += gridDim.x, ++item_ctr) {
+    const Rho1WorkItem W = P.items[it];
+    const int nc = W.nc, pn = W.pn, ncp = (nc + 3) & ~3;
+    const int ip = item_ctr & 1;
+    if (!mbar_wait(&S.sa_full[ip], (item_ctr >> 1) & 1, abort_flag, err)) return;
+    const double sA = S.scaleA[ip][p];
+    const long long col = W.wave_off + (long long)(W.p0 + p) * ncp;
+    const double *phi = P.wave + col;
+    const double *gph = P.gwave + 3 * W.wave_off + 3LL * (W.p0 + p) * ncp;
+    const int n_nt = (nc + SP_N - 1) / SP_N;
+    for (int t = 0; t < P.T; ++t) {
+      double r = 0.0, gx = 0.0, gy = 0.0, gz = 0.0;
+      for (int jn = 0; jn < n_nt; ++jn, ++tile_ctr) {
+        const int tp = tile_ctr & 1;
+        if (!mbar_wait(&S.sb_full[tp], (tile_ctr >> 1) & 1, abort_flag, err)) return;
+        if (!mbar_wait(&S.acc_full, tile_ctr & 1, abort_flag, err)) return;
+        tc_fence_after();
+#pragma unroll 1
+        for (int c0 = 0; c0 < SP_N; c0 += 16) {
+          float v0[16], v1[16], v2[16], v3[16];
+          tmem_ld16(lane_base + 0 * SP_N + c0, v0);
+          tmem_ld16(lane_base + 1 * SP_N + c0, v1);
+          tmem_ld16(lane_base + 2 * SP_N + c0, v2);
+          tmem_ld16(lane_base + 3 * SP_N + c0, v3);
+          tmem_wait_ld();
+          if (p < pn) {
+            const int ibase = jn * SP_N + c0;
+            const int jmax = min(16, nc - ibase);
+#pragma unroll 4
+            for (int j = 0; j < jmax; ++j) {
+              const int i = ibase + j;
+              const double w = sA * S.scaleB[tp][c0 + j] *
+                               (((double)v0[j] + (double)v1[j] + (double)v2[j]) + (double)v3[j]);
+              r += __ldg(phi + i) * w;
+              gx += __ldg(gph + i) * w;
+              gy += __ldg(gph + i + ncp) * w;
+              gz += __ldg(gph + i + 2 * ncp) * w;
+            }
+          }
+        }
+        tc_fence_before();
+        __syncwarp();
+        if (lane == 0) mbar_arrive(&S.acc_empty);
+      }
+      if (p < pn) {
+        const int pp = W.p0 + p;
+        const long long bidx = pp + (long long)P.n_max_batch_size * (W.batch + (long long)P.n_batches * t);
+        P.grad[3 * bidx + 0] = gx * 2 - P.gbias[3 * bidx + 0];
+        P.grad[3 * bidx + 1] = gy * 2 - P.gbias[3 * bidx + 1];
+        P.grad[3 * bidx + 2] = gz * 2 - P.gbias[3 * bidx + 2];
+        if (t < P.n_active) P.rho[P.map[W.prefix + pp] + (long long)P.n_full_points * t] = r + P.bias[bidx];
+      }
+    }
+  }
+}
+
+__global__ void __launch_bounds__(SP_THREADS, 1) rho1_split_kernel(const SplitParams P) {
+  extern __shared__ __align__(1024) unsigned char smem_raw[];
+  SplitSmem &S = *reinterpret_cast<SplitSmem *>(smem_raw);
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  if (tid == 0) {
+    for (int s = 0; s < SP_STAGES; ++s) {
+      mbar_init(&S.full[s], SP_PROD_WARPS);
+      mbar_init(&S.empty[s], 1);
+    }
+    mbar_init(&S.acc_full, 1);
+    mbar_init(&S.acc_empty, SP_EPI_WARPS);
+    mbar_init(&S.drain, 1);
+    for (int h = 0; h < 2; ++h) {
+      mbar_init(&S.sa_full[h], SP_PROD_THREADS / 4);
+      mbar_init(&S.sb_full[h], SP_PROD_THREADS / 4);
+    }
+    S.abort_flag = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == SP_MMA_WARP) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&S.tmem_base)),
+                 "r"(4 * SP_N));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = S.tmem_base;
+
+  if (warp < SP_EPI_WARPS) {
+    epilogue_role(P, S, tmem, warp, lane);
+  } else if (warp == SP_MMA_WARP) {
+    if (lane == 0) mma_role(P, S, tmem);
+    __syncwarp();
+  } else {
+    producer_role(P, S, tid - SP_PROD0 * 32, lane);
+  }
+
+  tc_fence_before();
+  __syncthreads();
+  if (warp == SP_MMA_WARP) {
+    tc_fence_after();
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(4 * SP_N));
+  }
+}
+
+// rowmax[r + n_basis t] = max_c |P1(r, c, t)|, the per-row scale of P1c
+// (an upper bound of the batch-local row maximum).
+__global__ void p1_rowmax_kernel(const double *__restrict__ P1, int n_basis, int cols_per_block,
+                                 unsigned long long *__restrict__ rowmax) {
+  const int r = blockIdx.x * blockDim.x + threadIdx.x;
+  const int t = blockIdx.z;
+  if (r >= n_basis) return;
+  const int c0 = blockIdx.y * cols_per_block, c1 = min(n_basis, c0 + cols_per_block);
+  const double *col = P1 + (long long)n_basis * n_basis * t + r;
+  double m = 0.0;
+  for (int c = c0; c < c1; ++c) m = fmax(m, fabs(col[(long long)c * n_basis]));
+  atomicMax(rowmax + r + (long long)n_basis * t, (unsigned long long)__double_as_longlong(m));
+}
+
+}  // namespace
+
+int rho1_split_smem_bytes() { return (int)sizeof(SplitSmem) + 1024; }
 
 int rho1_split_launch(const Rho1Plan &plan, int n_active, const double *wave, const double *gwave,
                       const double *P1, const double *bias, const double *gbias, double *rho, double *grad,
                       cudaStream_t stream) {
-  (void)plan; (void)n_active; (void)wave; (void)gwave; (void)P1; (void)bias; (void)gbias; (void)rho; (void)grad;
-  (void)stream;
-  return fail(FRPA_ERR_UNSUPPORTED, "rho1: split-BF16 mode not built yet");
+  if (plan.n_max_compute > SP_MAX_K)
+    return fail(FRPA_ERR_UNSUPPORTED,
+                "rho1 split-BF16: n_compute_c up to %d exceeds %d, the bound under which its exact FP32 levels "
+                "stay exact; use the FP64 mode",
+                plan.n_max_compute, SP_MAX_K);
+  FRPA_CUDA_TRY(cudaMemsetAsync(rho, 0, sizeof(double) * (size_t)plan.n_full_points * plan.T, stream));
+  FRPA_CUDA_TRY(cudaMemsetAsync(
+      grad, 0, sizeof(double) * 3 * (size_t)plan.n_max_batch_size * plan.n_batches * plan.T, stream));
+  if (plan.n_items_split == 0) return FRPA_OK;
+  // per-row scales of P1
+  FRPA_CUDA_TRY(cudaMemsetAsync(plan.d_rowmax, 0, sizeof(double) * (size_t)plan.n_basis * plan.T, stream));
+  const int cols = 256;
+  dim3 rg((plan.n_basis + 255) / 256, (plan.n_basis + cols - 1) / cols, plan.T);
+  p1_rowmax_kernel<<<rg, 256, 0, stream>>>(P1, plan.n_basis, cols,
+                                           reinterpret_cast<unsigned long long *>(plan.d_rowmax));
+  FRPA_LAUNCH_CHECK();
+  static int configured[64] = {0};
+  const int smem = rho1_split_smem_bytes();
+  if (plan.device >= 0 && plan.device < 64 && !configured[plan.device]) {
+    FRPA_CUDA_TRY(cudaFuncSetAttribute(rho1_split_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    configured[plan.device] = 1;
+  }
+  int n_sm = 148;
+  FRPA_CUDA_TRY(cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, plan.device));
+  SplitParams P;
+  P.items = plan.d_items_split;
+  P.n_items = plan.n_items_split;
+  P.ib_all = plan.d_ib;
+  P.map = plan.d_map;
+  P.T = plan.T;
+  P.n_active = n_active;
+  P.n_basis = plan.n_basis;
+  P.n_full_points = plan.n_full_points;
+  P.n_max_batch_size = plan.n_max_batch_size;
+  P.n_batches = plan.n_batches;
+  P.wave = wave;
+  P.gwave = gwave;
+  P.P1 = P1;
+  P.bias = bias;
+  P.gbias = gbias;
+  P.rowmax = plan.d_rowmax;
+  P.rho = rho;
+  P.grad = grad;
+  P.err = plan.d_err;
+  const int grid = std::min(n_sm, plan.n_items_split);
+  rho1_split_kernel<<<grid, SP_THREADS, smem, stream>>>(P);
+  FRPA_LAUNCH_CHECK();
+  return FRPA_OK;
+}
+
+// Work items of the split path: point tiles of <= 128 points, largest first.
+void rho1_split_build_items(const std::vector<Rho1WorkItem> &fp64_items, const int *np_b, int n_batches,
+                            std::vector<Rho1WorkItem> *out) {
+  (void)n_batches;
+  out->clear();
+  std::vector<int> seen;
+  for (const Rho1WorkItem &w : fp64_items) {
+    if (w.p0 != 0) continue;  // one entry per batch
+    const int np = np_b[w.batch];
+    const int tiles = (np + SP_M - 1) / SP_M;
+    const int width = (np + tiles - 1) / tiles;
+    for (int p0 = 0; p0 < np; p0 += width)
+      out->push_back(Rho1WorkItem{w.batch, w.nc, w.np, p0, std::min(width, np - p0), w.ib_off, w.prefix, 0,
+                                  w.wave_off});
+  }
+  std::stable_sort(out->begin(), out->end(), [](const Rho1WorkItem &a, const Rho1WorkItem &b) {
+    return (long long)a.nc * a.nc * a.pn > (long long)b.nc * b.nc * b.pn;
+  });
 }
 
 }  // namespace frpa

@@ -218,6 +218,11 @@ int frpa_rho1_execute(const frpa_rho1_plan *plan, int mode, int n_active, const 
 int frpa_rho1_adjoint_p1(const frpa_rho1_plan *plan, int n_active, const double *wave, const double *gradient_wave,
                          const double *g_rho, const double *g_grad, double *dP1, void *stream);
 
+/* Reads and clears the device-side status of the plan's split-BF16 kernel:
+ * bit 1 = a pipeline wait timed out (the kernel gave up and left its outputs
+ * incomplete), bit 2 = its final drain timed out.  0 after a good run. */
+int frpa_rho1_device_flags(const frpa_rho1_plan *plan, int *flags);
+
 typedef struct frpa_sumup_plan frpa_sumup_plan;
 
 /* Constant sum-up inputs (host arrays, reference layouts and meanings). */
