@@ -445,16 +445,35 @@ def run_frpa(args, ranks: Ranks):
     fp64_peak = _lib.probe_fp64_tflops("mma")
     fma_peak = _lib.probe_fp64_tflops("fma")
 
+    # both rho1 paths are timed on the same inputs; the headline is --mode
     clocks = ClockSampler(ranks.local)
     clocks.start()
-    ms = time_device_steps(lambda: w.step(mode, stream), args.steps, args.warmup, ranks, stream)
-    ms_fp64 = ms if mode == _lib.RHO1_FP64 else time_device_steps(
-        lambda: w.step(_lib.RHO1_FP64, stream), args.steps, args.warmup, ranks, stream)
+    ms_fp64 = time_device_steps(lambda: w.step(_lib.RHO1_FP64, stream), args.steps, args.warmup, ranks, stream)
+    ms_split = time_device_steps(lambda: w.step(_lib.RHO1_SPLIT_BF16, stream), args.steps, args.warmup, ranks,
+                                 stream)
     clk = clocks.stop()
+    ms = ms_fp64 if mode == _lib.RHO1_FP64 else ms_split
 
     total_pts = ranks.sum(float(w.points))
     value = total_pts / (ms / 1e3)
     achieved_tf = w.flops / (ms_fp64 / 1e3) / 1e12
+
+    # split-BF16 against plain FP64 on the full workload, same inputs
+    w.step(_lib.RHO1_SPLIT_BF16, stream)
+    torch.cuda.synchronize()
+    rho_m, grad_m = w.rho.clone(), w.grad.clone()
+    w.step(_lib.RHO1_FP64, stream)
+    torch.cuda.synchronize()
+    out["split_vs_fp64_normwise_rel"] = {
+        "rho1": float((rho_m - w.rho).abs().max() / w.rho.abs().max()),
+        "grad_rho1": float((grad_m - w.grad).abs().max() / w.grad.abs().max())}
+    out["device_flags"] = w.plan.device_flags()
+    del rho_m, grad_m
+    out["rho1_split_bf16"] = {"pts_per_s": total_pts / (ms_split / 1e3), "ms_per_step": ms_split,
+                              "speedup_vs_fp64": ms_fp64 / ms_split,
+                              "hbm_gbs_algorithmic": w_bytes / (ms_split / 1e3) / 1e9,
+                              "frac_of_measured_hbm": w_bytes / (ms_split / 1e3) / 1e9 / peaks["hbm_gbs"],
+                              "bf16_equivalent_tflops": 15 * w_flops / (ms_split / 1e3) / 1e12}
     out["rho1_fp64"] = {"pts_per_s": total_pts / (ms_fp64 / 1e3), "ms_per_step": ms_fp64,
                         "tflops_fp64": achieved_tf, "frac_of_measured_fp64_mma": achieved_tf / fp64_peak,
                         "hbm_gbs_algorithmic": w.bytes / (ms_fp64 / 1e3) / 1e9}
@@ -521,25 +540,36 @@ def run_frpa(args, ranks: Ranks):
             del sp
     out["sumup_config3"] = sumup
 
-    traffic = profile_traffic("rho1_fp64_kernel")
+    if mode == _lib.RHO1_FP64:
+        roofline = {"bound": "tensor", "achieved": achieved_tf, "peak": fp64_peak, "unit": "TFLOP/s",
+                    "frac": achieved_tf / fp64_peak, "traffic": profile_traffic("rho1_fp64_kernel"),
+                    "kernel": "rho1_fp64_kernel",
+                    "peak_source": "measured on this GPU in this run: FP64 m8n8k4 MMA throughput probe "
+                                   "(no FP64 figure in MEASURED_PEAKS.json)",
+                    "algorithmic_flops_per_launch": w_flops,
+                    "hbm_frac_of_measured": (w_bytes / (ms_fp64 / 1e3) / 1e9) / peaks["hbm_gbs"]}
+    else:
+        gbs = w_bytes / (ms / 1e3) / 1e9
+        roofline = {"bound": "hbm", "achieved": gbs, "peak": peaks["hbm_gbs"], "unit": "GB/s",
+                    "frac": gbs / peaks["hbm_gbs"], "traffic": profile_traffic("rho1_split_kernel"),
+                    "kernel": "rho1_split_kernel", "peak_source": peaks["source"] + " (MEASURED_PEAKS.json hbm_gbs)",
+                    "algorithmic_bytes_per_launch": w_bytes,
+                    "bf16_equivalent_tflops": 15 * w_flops / (ms / 1e3) / 1e12,
+                    "bf16_frac_of_measured": 15 * w_flops / (ms / 1e3) / 1e12 / peaks["bf16_tflops"]}
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-        "dtype": "f64", "data": "synthetic (seeded config-2 recipe: Gaussian x Y_lm basis, phi generated on the GPU)",
+        "dtype": "f64" if mode == _lib.RHO1_FP64 else "f64 in/out, bf16x5 slices -> f32 (tcgen05) contraction",
+        "data": "synthetic (seeded config-2 recipe: Gaussian x Y_lm basis, phi generated on the GPU)",
         "config": {"workload": "config2: rho1 + grad rho1, 1000 atoms at 0.1/A^3, 10 functions/atom, "
                                f"{p.n_my_batches_work} batches of 100-300 points, n_compute 100-600, T=1",
                    "path": mode_name, "valid_batches": info["n_valid_batches"], "work_items": info["n_items"],
                    "grid_points_per_rank": w_points,
                    "l2": "inputs larger than L2 (phi + grad phi = %.1f GB per rank)" % (4 * 8 * p.wave_len / 1e9),
                    "parallelism": f"weak, {args.gpus} independent shards"},
-        "roofline": {"bound": "tensor", "achieved": achieved_tf, "peak": fp64_peak, "unit": "TFLOP/s",
-                     "frac": achieved_tf / fp64_peak, "traffic": traffic,
-                     "peak_source": "measured on this GPU in this run: FP64 m8n8k4 MMA throughput probe "
-                                    "(no FP64 figure in MEASURED_PEAKS.json)",
-                     "algorithmic_flops_per_launch": w_flops,
-                     "hbm_frac_of_measured": (w_bytes / (ms_fp64 / 1e3) / 1e9) / peaks["hbm_gbs"]},
+        "roofline": roofline,
         "clocks": clk,
-        "gpu_launches": args.steps,
+        "gpu_launches": args.steps * (1 if mode == _lib.RHO1_FP64 else 2),
         "cpu_baseline": cpu,
         "e2e": e2e,
         "measured_fp64_tflops": {"mma": fp64_peak, "fma": fma_peak},

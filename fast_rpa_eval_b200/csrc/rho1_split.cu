@@ -22,7 +22,7 @@
 // typical size.  Only levels 3-4, 2^-24 below the result, see the tensor core's
 // FP32 truncation.  The benchmark recipes give normwise errors of ~2e-11.
 //
-// Data flow (one persistent CTA per SM, warp-specialised, 416 threads):
+// Data flow (one persistent CTA per SM, warp-specialised, 512 threads):
 //   * a work item is one batch's tile of <= 128 points; the MMA computes
 //     D[p, i] = sum_k Phi^T[p, k] P1c^T[k, i] (M = 128 points, N = 128 rows i,
 //     K = 16 per instruction), so each TMEM lane is one grid point and the
@@ -30,10 +30,13 @@
 //   * 8 producer warps read phi (FP64) and gather P1c (FP64), scale, split and
 //     store the 10 slice tiles of a 32-wide K chunk in shared memory
 //     (canonical K-major layout, no swizzle) -- a two-stage ring;
-//   * 1 warp owns TMEM (512 columns = 4 accumulators x 128) and issues the
-//     15 x 2 tcgen05.mma per stage, committing to mbarriers;
-//   * 4 epilogue warps read the accumulators (tcgen05.ld), recombine in FP64
-//     and contract with phi and grad phi (FP64, global memory).
+//   * epilogue warp 0 owns TMEM (512 columns = 4 accumulators x 128) and its
+//     lane 0 issues the 15 x 2 tcgen05.mma per stage, committing to mbarriers
+//     (with one accumulator set, a tile's MMAs and its epilogue never overlap);
+//   * 8 epilogue warps (two per TMEM lane quarter, each taking half of the
+//     columns) read the accumulators (tcgen05.ld), recombine in FP64 and
+//     contract with phi and grad phi (FP64, global memory, loads issued a
+//     chunk ahead).
 // Every mbarrier wait is bounded in time; on a timeout the kernel records an
 // error flag, lets in-flight MMAs finish (bounded), frees TMEM and returns.
 #include <cuda_bf16.h>
@@ -51,11 +54,11 @@ constexpr int SP_N = 128;         // rows i per N tile (accumulator columns)
 constexpr int SP_KC = 32;         // K per pipeline stage
 constexpr int SP_STAGES = 2;
 constexpr int SP_SLICES = 5;
-constexpr int SP_EPI_WARPS = 4;   // warps 0..3: epilogue (TMEM lanes 0..127)
-constexpr int SP_MMA_WARP = 4;    // warp 4: TMEM owner and MMA issuer
-constexpr int SP_PROD_WARPS = 8;  // warps 5..12: producers
-constexpr int SP_PROD0 = SP_MMA_WARP + 1;
-constexpr int SP_THREADS = 32 * (SP_EPI_WARPS + 1 + SP_PROD_WARPS);
+constexpr int SP_EPI_WARPS = 8;   // warps 0..7: epilogue (lane quarter w % 4, column half w / 4);
+                                  // warp 0 owns TMEM and its lane 0 issues the MMAs
+constexpr int SP_PROD_WARPS = 8;  // warps 8..15: producers
+constexpr int SP_PROD0 = SP_EPI_WARPS;
+constexpr int SP_THREADS = 32 * (SP_EPI_WARPS + SP_PROD_WARPS);
 constexpr int SP_PROD_THREADS = 32 * SP_PROD_WARPS;
 constexpr int SP_MAX_K = 1024;    // exactness bound of the FP32 levels 0 and 1
 constexpr int SP_TILE_ELEMS = SP_M * SP_KC;           // one slice tile (bf16 elements)
@@ -69,9 +72,8 @@ struct SplitSmem {
   __nv_bfloat16 A[SP_STAGES][SP_SLICES][SP_TILE_ELEMS];
   __nv_bfloat16 B[SP_STAGES][SP_SLICES][SP_TILE_ELEMS];
   double scaleA[2][SP_M];  // 2^(eA - 7) per point, by item parity
-  double invA[2][SP_M];    // 2^-eA
   double scaleB[2][SP_N];  // 2^(eB - 7) per row i, by tile parity
-  double invB[2][SP_N];
+  double partial[2][4][SP_M];  // upper column half's per-point sums
   unsigned long long full[SP_STAGES];
   unsigned long long empty[SP_STAGES];
   unsigned long long acc_full;
@@ -79,6 +81,10 @@ struct SplitSmem {
   unsigned long long drain;
   unsigned long long sa_full[2];  // per-point scales of an item published (by item parity)
   unsigned long long sb_full[2];  // per-row scales of a tile published (by tile parity)
+  unsigned long long sa_free[2];  // per-point scales released by the epilogue
+  unsigned long long sb_free[2];  // per-row scales released by the epilogue
+  unsigned long long ep_sum[2];   // partial sums published by the upper column half
+  unsigned long long ep_free[2];  // partial-sum buffer released by the lower half
   uint32_t tmem_base;
   int abort_flag;
 };
@@ -132,6 +138,18 @@ __device__ __forceinline__ bool mbar_wait(unsigned long long *bar, uint32_t pari
   }
 }
 
+// Warp-uniform bounded wait: lane 0 polls, the outcome goes to every lane,
+// so a warp never splits over a timeout; __syncwarp orders the lanes' later
+// reads after lane 0's acquire.
+__device__ __forceinline__ bool warp_wait(unsigned long long *bar, uint32_t parity, volatile int *abort_flag,
+                                          int *err, int lane) {
+  int ok = 1;
+  if (lane == 0) ok = mbar_wait(bar, parity, abort_flag, err) ? 1 : 0;
+  ok = __shfl_sync(0xffffffffu, ok, 0);
+  __syncwarp();
+  return ok != 0;
+}
+
 __device__ __forceinline__ void fence_proxy_async_smem() {
   asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
 }
@@ -171,33 +189,6 @@ __device__ __forceinline__ void umma_bf16(uint32_t d_tmem, uint64_t a_desc, uint
 __device__ __forceinline__ void umma_commit(unsigned long long *bar) {
   asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
                : "memory");
-}
-
-__device__ __forceinline__ void tmem_ld32(uint32_t taddr, float (&v)[32]) {
-  uint32_t r[32];
-  asm volatile(
-      "tcgen05.ld.sync.aligned.32x32b.x32.b32 "
-      "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
-      "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
-      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
-        "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]),
-        "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]),
-        "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
-      : "r"(taddr));
-#pragma unroll
-  for (int j = 0; j < 32; ++j) v[j] = __uint_as_float(r[j]);
-}
-
-__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16]) {
-  uint32_t r[16];
-  asm volatile(
-      "tcgen05.ld.sync.aligned.32x32b.x16.b32 "
-      "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
-      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
-        "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
-      : "r"(taddr));
-#pragma unroll
-  for (int j = 0; j < 16; ++j) v[j] = __uint_as_float(r[j]);
 }
 
 __device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
@@ -255,9 +246,40 @@ struct SplitParams {
 // (row, kseg) = ((q & 7) + 8 (q >> 5), (q >> 3) & 3): a quarter warp stores
 // eight rows' 16-byte chunks of one core-matrix column (conflict-free), and
 // the four lanes sharing a row are lanes l, l^8, l^16, l^24 of one warp.
+// Each producer thread owns segments ptid and ptid + 256 (rows r and r + 64,
+// same kseg) of both operand tiles.
 __device__ __forceinline__ void seg_of(int q, int *row, int *kseg) {
   *row = (q & 7) + 8 * (q >> 5);
   *kseg = (q >> 3) & 3;
+}
+
+// Raw FP64 operands of one stage for one producer thread (2 rows x 8 k).
+struct StageRegs {
+  double a[2][8];
+  double b[2][8];
+};
+
+__device__ __forceinline__ void load_a(StageRegs &R, const double *__restrict__ phi, int ncp, int nc, int pn,
+                                       const int (&rows)[2], int k) {
+#pragma unroll
+  for (int h = 0; h < 2; ++h)
+#pragma unroll
+    for (int j = 0; j < 8; ++j)
+      R.a[h][j] = (rows[h] < pn && k + j < nc) ? __ldg(phi + k + j + (long long)rows[h] * ncp) : 0.0;
+}
+
+__device__ __forceinline__ void load_b(StageRegs &R, const double *__restrict__ P1t, int n_basis, int nc,
+                                       const int (&ibrow)[2], const bool (&rok)[2], const int (&ibk)[8]) {
+#pragma unroll
+  for (int h = 0; h < 2; ++h)
+#pragma unroll
+    for (int j = 0; j < 8; ++j)
+      R.b[h][j] = (rok[h] && ibk[j] >= 0) ? __ldg(P1t + ibrow[h] + (long long)ibk[j] * n_basis) : 0.0;
+}
+
+__device__ __forceinline__ void load_ibk(int (&ibk)[8], const int *__restrict__ ib, int nc, int k) {
+#pragma unroll
+  for (int j = 0; j < 8; ++j) ibk[j] = (k + j < nc) ? __ldg(ib + k + j) - 1 : -1;
 }
 
 __device__ void producer_role(const SplitParams &P, SplitSmem &S, int ptid, int lane) {
@@ -265,195 +287,279 @@ __device__ void producer_role(const SplitParams &P, SplitSmem &S, int ptid, int 
   volatile int *abort_flag = &S.abort_flag;
   const long long nb2 = (long long)P.n_basis * P.n_basis;
   uint32_t fill = 0, tile_ctr = 0, item_ctr = 0;
-  int rows[2], ksegs[2];
-  seg_of(ptid, &rows[0], &ksegs[0]);
-  seg_of(ptid + SP_PROD_THREADS, &rows[1], &ksegs[1]);
+  int rows[2], kseg;
+  seg_of(ptid, &rows[0], &kseg);
+  rows[1] = rows[0] + 64;
   for (int it = blockIdx.x; it < P.n_items; it += gridDim.x, ++item_ctr) {
     const Rho1WorkItem W = P.items[it];
     const int nc = W.nc, pn = W.pn, ncp = (nc + 3) & ~3;
     const double *phi = P.wave + W.wave_off + (long long)W.p0 * ncp;
     const int *ib = P.ib_all + W.ib_off;
     const int ip = item_ctr & 1;
+    // the epilogue is done with this parity's scales of two items ago
+    if (!warp_wait(&S.sa_free[ip], ((item_ctr >> 1) & 1) ^ 1, abort_flag, err, lane)) return;
     // per-point scales: the four lanes sharing a row split its column
     double invA[2];
 #pragma unroll
     for (int h = 0; h < 2; ++h) {
       const int r = rows[h];
       double m = 0.0;
-      if (r < pn)
-        for (int k = ksegs[h]; k < nc; k += 4) m = fmax(m, fabs(phi[k + (long long)r * ncp]));
+      if (r < pn) {
+        const double *c = phi + (long long)r * ncp;
+#pragma unroll 4
+        for (int k = kseg; k < nc; k += 4) m = fmax(m, fabs(__ldg(c + k)));
+      }
       m = fmax(m, __shfl_xor_sync(0xffffffffu, m, 8));
       m = fmax(m, __shfl_xor_sync(0xffffffffu, m, 16));
       double sc;
       pow2_scale(m, &sc, &invA[h]);
-      if (ksegs[h] == 0) S.scaleA[ip][r] = sc;
+      if (kseg == 0) S.scaleA[ip][r] = sc;
     }
-    if (ksegs[0] == 0) mbar_arrive(&S.sa_full[ip]);
+    if (kseg == 0) mbar_arrive(&S.sa_full[ip]);
     const int n_nt = (nc + SP_N - 1) / SP_N, n_kc = (nc + SP_KC - 1) / SP_KC;
-    for (int t = 0; t < P.T; ++t) {
+    const int n_stages = P.T * n_nt * n_kc;  // flattened (t, jn, kc)
+    StageRegs R;
+    int ibk[8], ibrow[2];
+    bool rok[2];
+    double invB[2];
+    // prologue: operands of the item's first stage
+    load_ibk(ibk, ib, nc, 8 * kseg);
+    load_a(R, phi, ncp, nc, pn, rows, 8 * kseg);
+    for (int st = 0; st < n_stages; ++st, ++fill) {
+      const int kc = st % n_kc, jn = (st / n_kc) % n_nt, t = st / (n_kc * n_nt);
       const double *P1t = P.P1 + t * nb2;
-      for (int jn = 0; jn < n_nt; ++jn, ++tile_ctr) {
+      if (kc == 0) {
+        // a new N tile: its per-row scales (buffer released by the epilogue)
         const int n0 = jn * SP_N, tp = tile_ctr & 1;
-        double invB[2];
-        int ibrow[2];
+        if (!warp_wait(&S.sb_free[tp], ((tile_ctr >> 1) & 1) ^ 1, abort_flag, err, lane)) return;
 #pragma unroll
         for (int h = 0; h < 2; ++h) {
           const int i = n0 + rows[h];
-          ibrow[h] = i < nc ? ib[i] - 1 : 0;
-          const double m = i < nc ? P.rowmax[ibrow[h] + (long long)P.n_basis * t] : 0.0;
+          rok[h] = i < nc;
+          ibrow[h] = rok[h] ? __ldg(ib + i) - 1 : 0;
+          const double m = rok[h] ? __ldg(P.rowmax + ibrow[h] + (long long)P.n_basis * t) : 0.0;
           double sc;
           pow2_scale(m, &sc, &invB[h]);
-          if (ksegs[h] == 0) S.scaleB[tp][rows[h]] = sc;
+          if (kseg == 0) S.scaleB[tp][rows[h]] = sc;
         }
-        if (ksegs[0] == 0) mbar_arrive(&S.sb_full[tp]);
-        for (int kc = 0; kc < n_kc; ++kc, ++fill) {
-          const int stage = fill & 1;
-          const uint32_t use = fill >> 1;
-          if (!mbar_wait(&S.empty[stage], (use & 1) ^ 1, abort_flag, err)) return;
-          const int k0 = kc * SP_KC;
-#pragma unroll
-          for (int h = 0; h < 2; ++h) {
-            const int r = rows[h], k = k0 + 8 * ksegs[h];
-            double y[8];
-            // A = Phi^T: row = point r, columns k..k+7
-#pragma unroll
-            for (int j = 0; j < 8; ++j)
-              y[j] = (r < pn && k + j < nc) ? phi[k + j + (long long)r * ncp] * invA[h] : 0.0;
-            split8_store(y, S.A[stage], tile_off(r, 8 * ksegs[h]));
-            // B = P1c (K-major): row i = n0 + r, columns k..k+7
-            const bool rok = n0 + r < nc;
-#pragma unroll
-            for (int j = 0; j < 8; ++j)
-              y[j] = (rok && k + j < nc) ? P1t[ibrow[h] + (long long)(ib[k + j] - 1) * P.n_basis] * invB[h] : 0.0;
-            split8_store(y, S.B[stage], tile_off(r, 8 * ksegs[h]));
-          }
-          fence_proxy_async_smem();
-          __syncwarp();
-          if (lane == 0) mbar_arrive(&S.full[stage]);
-        }
+        if (kseg == 0) mbar_arrive(&S.sb_full[tp]);
+        ++tile_ctr;
       }
+      load_b(R, P1t, P.n_basis, nc, ibrow, rok, ibk);
+      const int stage = fill & 1;
+      if (!warp_wait(&S.empty[stage], ((fill >> 1) & 1) ^ 1, abort_flag, err, lane)) return;
+      // A half: convert, then start the next stage's A loads
+      const int koff = 8 * kseg;
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        double y[8];
+#pragma unroll
+        for (int j = 0; j < 8; ++j) y[j] = R.a[h][j] * invA[h];
+        split8_store(y, S.A[stage], tile_off(rows[h], koff));
+      }
+      const bool more = st + 1 < n_stages;
+      if (more) {
+        const int k1 = ((st + 1) % n_kc) * SP_KC + koff;
+        load_ibk(ibk, ib, nc, k1);
+        load_a(R, phi, ncp, nc, pn, rows, k1);
+      }
+      // B half
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        double y[8];
+#pragma unroll
+        for (int j = 0; j < 8; ++j) y[j] = R.b[h][j] * invB[h];
+        split8_store(y, S.B[stage], tile_off(rows[h], koff));
+      }
+      fence_proxy_async_smem();
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&S.full[stage]);
     }
   }
 }
 
-__device__ void mma_role(const SplitParams &P, SplitSmem &S, uint32_t tmem) {
-  int *err = P.err;
-  volatile int *abort_flag = &S.abort_flag;
-  uint32_t fill = 0, tile_ctr = 0;
-  bool issued = false;
-  for (int it = blockIdx.x; it < P.n_items && !*abort_flag; it += gridDim.x) {
-    const int nc = P.items[it].nc;
-    const int n_nt = (nc + SP_N - 1) / SP_N, n_kc = (nc + SP_KC - 1) / SP_KC;
-    for (int t = 0; t < P.T; ++t)
-      for (int jn = 0; jn < n_nt; ++jn, ++tile_ctr) {
-        if (!mbar_wait(&S.acc_empty, (tile_ctr & 1) ^ 1, abort_flag, err)) goto done;
-        tc_fence_after();
-        for (int kc = 0; kc < n_kc; ++kc, ++fill) {
-          const int stage = fill & 1;
-          if (!mbar_wait(&S.full[stage], (fill >> 1) & 1, abort_flag, err)) goto done;
-          tc_fence_after();
+// Issues one N tile's MMAs (all K stages) from a single thread.  With one
+// accumulator set in TMEM the MMAs of a tile never overlap that tile's
+// epilogue, so the issuing thread is lane 0 of epilogue warp 0.
+__device__ bool mma_tile(SplitSmem &S, uint32_t tmem, int n_kc, uint32_t &fill, uint32_t tile_ctr,
+                         volatile int *abort_flag, int *err) {
+  if (!mbar_wait(&S.acc_empty, (tile_ctr & 1) ^ 1, abort_flag, err)) return false;
+  tc_fence_after();
+  for (int kc = 0; kc < n_kc; ++kc, ++fill) {
+    const int stage = fill & 1;
+    if (!mbar_wait(&S.full[stage], (fill >> 1) & 1, abort_flag, err)) return false;
+    tc_fence_after();
 #pragma unroll
-          for (int ks = 0; ks < SP_KC / 16; ++ks) {
-            uint64_t a[SP_SLICES], b[SP_SLICES];
+    for (int ks = 0; ks < SP_KC / 16; ++ks) {
+      uint64_t a[SP_SLICES], b[SP_SLICES];
 #pragma unroll
-            for (int s = 0; s < SP_SLICES; ++s) {
-              a[s] = smem_desc(smem_u32(S.A[stage][s]) + ks * 2 * SP_LBO);
-              b[s] = smem_desc(smem_u32(S.B[stage][s]) + ks * 2 * SP_LBO);
-            }
-            const uint32_t acc = (kc > 0 || ks > 0) ? 1u : 0u;
-            // accumulator q holds slice level s + u = q (q < 3, exact) and the
-            // levels 3 and 4 (q = 3, rounded)
-            uint32_t first[4] = {acc, acc, acc, acc};
+      for (int s = 0; s < SP_SLICES; ++s) {
+        a[s] = smem_desc(smem_u32(S.A[stage][s]) + ks * 2 * SP_LBO);
+        b[s] = smem_desc(smem_u32(S.B[stage][s]) + ks * 2 * SP_LBO);
+      }
+      const uint32_t acc = (kc > 0 || ks > 0) ? 1u : 0u;
+      // accumulator q holds slice level s + u = q (q < 3, exact) and the
+      // levels 3 and 4 (q = 3, rounded)
+      uint32_t first[4] = {acc, acc, acc, acc};
 #pragma unroll
-            for (int s = 0; s < SP_SLICES; ++s)
+      for (int s = 0; s < SP_SLICES; ++s)
 #pragma unroll
-              for (int u = 0; u < SP_SLICES; ++u)
-                if (s + u <= 4) {
-                  const int q = s + u < 3 ? s + u : 3;
-                  umma_bf16(tmem + q * SP_N, a[s], b[u], first[q]);
-                  first[q] = 1u;
-                }
+        for (int u = 0; u < SP_SLICES; ++u)
+          if (s + u <= 4) {
+            const int q = s + u < 3 ? s + u : 3;
+            umma_bf16(tmem + q * SP_N, a[s], b[u], first[q]);
+            first[q] = 1u;
           }
-          umma_commit(&S.empty[stage]);
-          issued = true;
-        }
-        umma_commit(&S.acc_full);
-      }
+    }
+    umma_commit(&S.empty[stage]);
   }
-done:
-  if (issued) {
-    // every MMA issued by this thread has completed once this commit arrives
-    umma_commit(&S.drain);
-    const unsigned long long t0 = global_ns();
-    while (!mbar_try_wait(&S.drain, 0)) {
-      if (global_ns() - t0 > SP_WAIT_NS) {
-        atomicOr(err, 4);
-        break;
-      }
+  umma_commit(&S.acc_full);
+  return true;
+}
+
+// Waits (bounded) until every MMA issued so far by this thread has completed.
+__device__ void mma_drain(SplitSmem &S, int *err) {
+  umma_commit(&S.drain);
+  const unsigned long long t0 = global_ns();
+  while (!mbar_try_wait(&S.drain, 0)) {
+    if (global_ns() - t0 > SP_WAIT_NS) {
+      atomicOr(err, 4);
+      break;
     }
   }
 }
 
-__device__ void epilogue_role(const SplitParams &P, SplitSmem &S, uint32_t tmem, int warp, int lane) {
+__device__ __forceinline__ void tmem_ld8(uint32_t taddr, float (&v)[8]) {
+  uint32_t r[8];
+  asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
+               : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7])
+               : "r"(taddr));
+#pragma unroll
+  for (int j = 0; j < 8; ++j) v[j] = __uint_as_float(r[j]);
+}
+
+// FP64 operands of one 8-column chunk of the epilogue: phi and grad phi at
+// rows i = i0..i0+7 of one point's column (zero past n_compute).
+struct EpiRegs {
+  double f[8], gx[8], gy[8], gz[8];
+};
+
+__device__ __forceinline__ void epi_load(EpiRegs &E, const double *__restrict__ phi, const double *__restrict__ gph,
+                                         int ncp, int nc, int i0, bool live) {
+#pragma unroll
+  for (int j = 0; j < 8; ++j) {
+    const bool ok = live && i0 + j < nc;
+    E.f[j] = ok ? __ldg(phi + i0 + j) : 0.0;
+    E.gx[j] = ok ? __ldg(gph + i0 + j) : 0.0;
+    E.gy[j] = ok ? __ldg(gph + i0 + j + ncp) : 0.0;
+    E.gz[j] = ok ? __ldg(gph + i0 + j + 2 * ncp) : 0.0;
+  }
+}
+
+// Epilogue warp w reads TMEM lanes 32 (w % 4).. (its points) and accumulator
+// columns 64 (w / 4)..+63 of every N tile; the two warps sharing a lane
+// quarter add their partial sums through shared memory at each perturbation's
+// end (the upper half publishes through ep_sum, the lower half writes the
+// outputs and releases the buffer through ep_free).
+__device__ void epilogue_body(const SplitParams &P, SplitSmem &S, uint32_t tmem, int warp, int lane, bool &issued) {
   int *err = P.err;
   volatile int *abort_flag = &S.abort_flag;
-  const int p = warp * 32 + lane;  // TMEM lane = point within the tile
-  const uint32_t lane_base = tmem + ((uint32_t)(warp * 32) << 16);
-  uint32_t tile_ctr = 0, item_ctr = 0;
+  const int quarter = warp & 3, half = warp >> 2;
+  const int p = quarter * 32 + lane;  // TMEM lane = point within the tile
+  const uint32_t lane_base = tmem + ((uint32_t)(quarter * 32) << 16);
+  const int cbase = half * (SP_N / 2);
+  uint32_t tile_ctr = 0, item_ctr = 0, sum_ctr = 0, fill = 0;
+  const bool issuer = warp == 0 && lane == 0;
   for (int it = blockIdx.x; it < P.n_items; it += gridDim.x, ++item_ctr) {
     const Rho1WorkItem W = P.items[it];
     const int nc = W.nc, pn = W.pn, ncp = (nc + 3) & ~3;
     const int ip = item_ctr & 1;
-    if (!mbar_wait(&S.sa_full[ip], (item_ctr >> 1) & 1, abort_flag, err)) return;
-    const double sA = S.scaleA[ip][p];
-    const long long col = W.wave_off + (long long)(W.p0 + p) * ncp;
-    const double *phi = P.wave + col;
+    const bool live = p < pn;
+    const int n_kc = (nc + SP_KC - 1) / SP_KC;
+    const double *phi = P.wave + W.wave_off + (long long)(W.p0 + p) * ncp;
     const double *gph = P.gwave + 3 * W.wave_off + 3LL * (W.p0 + p) * ncp;
+    if (!warp_wait(&S.sa_full[ip], (item_ctr >> 1) & 1, abort_flag, err, lane)) return;
+    const double sA = S.scaleA[ip][p];
+    __syncwarp();
+    if (lane == 0) mbar_arrive(&S.sa_free[ip]);
     const int n_nt = (nc + SP_N - 1) / SP_N;
     for (int t = 0; t < P.T; ++t) {
       double r = 0.0, gx = 0.0, gy = 0.0, gz = 0.0;
       for (int jn = 0; jn < n_nt; ++jn, ++tile_ctr) {
         const int tp = tile_ctr & 1;
-        if (!mbar_wait(&S.sb_full[tp], (tile_ctr >> 1) & 1, abort_flag, err)) return;
-        if (!mbar_wait(&S.acc_full, tile_ctr & 1, abort_flag, err)) return;
+        const int ibase = jn * SP_N + cbase;
+        EpiRegs E;
+        epi_load(E, phi, gph, ncp, nc, ibase, live);  // independent of the MMA: before the wait
+        if (issuer) {
+          issued = true;
+          mma_tile(S, tmem, n_kc, fill, tile_ctr, abort_flag, err);  // a failure sets abort_flag
+        }
+        __syncwarp();
+        if (*abort_flag) return;
+        if (!warp_wait(&S.sb_full[tp], (tile_ctr >> 1) & 1, abort_flag, err, lane)) return;
+        if (!warp_wait(&S.acc_full, tile_ctr & 1, abort_flag, err, lane)) return;
         tc_fence_after();
 #pragma unroll 1
-        for (int c0 = 0; c0 < SP_N; c0 += 16) {
-          float v0[16], v1[16], v2[16], v3[16];
-          tmem_ld16(lane_base + 0 * SP_N + c0, v0);
-          tmem_ld16(lane_base + 1 * SP_N + c0, v1);
-          tmem_ld16(lane_base + 2 * SP_N + c0, v2);
-          tmem_ld16(lane_base + 3 * SP_N + c0, v3);
+        for (int c = 0; c < SP_N / 2; c += 8) {
+          float v0[8], v1[8], v2[8], v3[8];
+          tmem_ld8(lane_base + 0 * SP_N + cbase + c, v0);
+          tmem_ld8(lane_base + 1 * SP_N + cbase + c, v1);
+          tmem_ld8(lane_base + 2 * SP_N + cbase + c, v2);
+          tmem_ld8(lane_base + 3 * SP_N + cbase + c, v3);
           tmem_wait_ld();
-          if (p < pn) {
-            const int ibase = jn * SP_N + c0;
-            const int jmax = min(16, nc - ibase);
-#pragma unroll 4
-            for (int j = 0; j < jmax; ++j) {
-              const int i = ibase + j;
-              const double w = sA * S.scaleB[tp][c0 + j] *
-                               (((double)v0[j] + (double)v1[j] + (double)v2[j]) + (double)v3[j]);
-              r += __ldg(phi + i) * w;
-              gx += __ldg(gph + i) * w;
-              gy += __ldg(gph + i + ncp) * w;
-              gz += __ldg(gph + i + 2 * ncp) * w;
-            }
+#pragma unroll
+          for (int j = 0; j < 8; ++j) {
+            const double w = sA * S.scaleB[tp][cbase + c + j] *
+                             (((double)v0[j] + (double)v1[j] + (double)v2[j]) + (double)v3[j]);
+            r += E.f[j] * w;
+            gx += E.gx[j] * w;
+            gy += E.gy[j] * w;
+            gz += E.gz[j] * w;
           }
+          if (c + 8 < SP_N / 2) epi_load(E, phi, gph, ncp, nc, ibase + c + 8, live);
         }
         tc_fence_before();
         __syncwarp();
-        if (lane == 0) mbar_arrive(&S.acc_empty);
+        if (lane == 0) {
+          mbar_arrive(&S.sb_free[tp]);
+          mbar_arrive(&S.acc_empty);
+        }
       }
-      if (p < pn) {
-        const int pp = W.p0 + p;
-        const long long bidx = pp + (long long)P.n_max_batch_size * (W.batch + (long long)P.n_batches * t);
-        P.grad[3 * bidx + 0] = gx * 2 - P.gbias[3 * bidx + 0];
-        P.grad[3 * bidx + 1] = gy * 2 - P.gbias[3 * bidx + 1];
-        P.grad[3 * bidx + 2] = gz * 2 - P.gbias[3 * bidx + 2];
-        if (t < P.n_active) P.rho[P.map[W.prefix + pp] + (long long)P.n_full_points * t] = r + P.bias[bidx];
+      // combine the two column halves of this point and write
+      const int sp = sum_ctr & 1;
+      if (half == 1) {
+        if (!warp_wait(&S.ep_free[sp], ((sum_ctr >> 1) & 1) ^ 1, abort_flag, err, lane)) return;
+        S.partial[sp][0][p] = r;
+        S.partial[sp][1][p] = gx;
+        S.partial[sp][2][p] = gy;
+        S.partial[sp][3][p] = gz;
+        mbar_arrive(&S.ep_sum[sp]);
+      } else {
+        if (!warp_wait(&S.ep_sum[sp], (sum_ctr >> 1) & 1, abort_flag, err, lane)) return;
+        r += S.partial[sp][0][p];
+        gx += S.partial[sp][1][p];
+        gy += S.partial[sp][2][p];
+        gz += S.partial[sp][3][p];
+        mbar_arrive(&S.ep_free[sp]);
+        if (live) {
+          const int pp = W.p0 + p;
+          const long long bidx = pp + (long long)P.n_max_batch_size * (W.batch + (long long)P.n_batches * t);
+          P.grad[3 * bidx + 0] = gx * 2 - P.gbias[3 * bidx + 0];
+          P.grad[3 * bidx + 1] = gy * 2 - P.gbias[3 * bidx + 1];
+          P.grad[3 * bidx + 2] = gz * 2 - P.gbias[3 * bidx + 2];
+          if (t < P.n_active) P.rho[P.map[W.prefix + pp] + (long long)P.n_full_points * t] = r + P.bias[bidx];
+        }
       }
+      ++sum_ctr;
     }
   }
+}
+
+__device__ void epilogue_role(const SplitParams &P, SplitSmem &S, uint32_t tmem, int warp, int lane) {
+  bool issued = false;
+  epilogue_body(P, S, tmem, warp, lane, issued);
+  // no MMA may be in flight when TMEM is released
+  if (issued) mma_drain(S, P.err);
 }
 
 __global__ void __launch_bounds__(SP_THREADS, 1) rho1_split_kernel(const SplitParams P) {
@@ -471,11 +577,15 @@ __global__ void __launch_bounds__(SP_THREADS, 1) rho1_split_kernel(const SplitPa
     for (int h = 0; h < 2; ++h) {
       mbar_init(&S.sa_full[h], SP_PROD_THREADS / 4);
       mbar_init(&S.sb_full[h], SP_PROD_THREADS / 4);
+      mbar_init(&S.sa_free[h], SP_EPI_WARPS);
+      mbar_init(&S.sb_free[h], SP_EPI_WARPS);
+      mbar_init(&S.ep_sum[h], SP_M);
+      mbar_init(&S.ep_free[h], SP_M);
     }
     S.abort_flag = 0;
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
-  if (warp == SP_MMA_WARP) {
+  if (warp == 0) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&S.tmem_base)),
                  "r"(4 * SP_N));
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
@@ -487,8 +597,6 @@ __global__ void __launch_bounds__(SP_THREADS, 1) rho1_split_kernel(const SplitPa
 
   if (warp < SP_EPI_WARPS) {
     epilogue_role(P, S, tmem, warp, lane);
-  } else if (warp == SP_MMA_WARP) {
-    if (lane == 0) mma_role(P, S, tmem);
     __syncwarp();
   } else {
     producer_role(P, S, tid - SP_PROD0 * 32, lane);
@@ -496,7 +604,7 @@ __global__ void __launch_bounds__(SP_THREADS, 1) rho1_split_kernel(const SplitPa
 
   tc_fence_before();
   __syncthreads();
-  if (warp == SP_MMA_WARP) {
+  if (warp == 0) {
     tc_fence_after();
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(4 * SP_N));
   }
