@@ -14,7 +14,8 @@ import threading
 import numpy as np
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(_HERE, "lib", "libfrpa.so")
+# FRPA_LIB overrides the library path (e.g. an alternative build of the same sources)
+LIB_PATH = os.environ.get("FRPA_LIB") or os.path.join(_HERE, "lib", "libfrpa.so")
 
 FRPA_OK = 0
 FRPA_ERR_INVALID = 1

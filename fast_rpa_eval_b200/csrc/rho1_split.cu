@@ -198,36 +198,65 @@ __device__ __forceinline__ int tile_off(int r, int k) {
   return (r >> 3) * SP_SBO + (k >> 3) * SP_LBO + (r & 7) * 16 + (k & 7) * 2;
 }
 
-// Five slices of 8 consecutive values (already scaled to [-1, 1]) written as
-// 16-byte rows into the slice tiles at byte offset `off`.
-__device__ __forceinline__ void split8_store(const double (&y)[8], __nv_bfloat16 (*tiles)[SP_TILE_ELEMS],
-                                             int off) {
-  double r[8];
+// Five slices of 8 consecutive raw values x (row scale folded into
+// sc39 = 2^(39 - e)) written as 16-byte rows into the slice tiles at byte
+// offset `off`.  Integer digit extraction, no FP64 rounding or conversion:
+//   t = fma(x, sc39, 1.5 2^52) rounds X = rint(y 2^39) into the mantissa:
+//       lo word = X mod 2^32, hi word & 0xFFFFF = 2^19 + floor(X / 2^32);
+//   X + 0x80808080 = a0 2^32 + sum_i c_i 2^(8 i), c_i bytes in [0, 255], so
+//       X = a0 2^32 + sum_i (c_i - 128) 2^(8 i): balanced digits d = c - 128;
+//   a digit c becomes the float (c - 128) 2^(-8 s) exactly as
+//       fma(bits(0x4B000000 | c), 2^(-8 s), -(2^23 + 128) 2^(-8 s)),
+//   and a float with <= 8 significant bits is exact in BF16: its top 16 bits.
+__device__ __forceinline__ void split8_store(const double (&x)[8], double sc39,
+                                             __nv_bfloat16 (*tiles)[SP_TILE_ELEMS], int off) {
+  uint32_t lo[8], f0[8];
 #pragma unroll
-  for (int j = 0; j < 8; ++j) r[j] = y[j] * 128.0;
-#pragma unroll
-  for (int s = 0; s < SP_SLICES; ++s) {
-    const float scale = (s == 0) ? 1.0f : __int_as_float((127 - 8 * s) << 23);  // 2^(-8 s)
+  for (int j = 0; j < 8; ++j) {
+    const double t = fma(x[j], sc39, 6755399441055744.0);  // 1.5 * 2^52
+    const uint32_t l = (uint32_t)__double2loint(t), h = (uint32_t)__double2hiint(t);
+    const uint32_t lp = l + 0x80808080u;
+    const uint32_t carry = lp < l ? 1u : 0u;
+    lo[j] = lp;
+    // bits of the float 2^23 + (a0 + 128), a0 = (h & 0xFFFFF) - 2^19 + carry
+    f0[j] = (h & 0xFFFFFu) + carry + (0x4B000000u + 128u - 0x80000u);
+  }
+  {
     uint32_t packed[4];
 #pragma unroll
     for (int j = 0; j < 8; j += 2) {
-      const double a0 = rint(r[j]), a1 = rint(r[j + 1]);
-      r[j] = (r[j] - a0) * 256.0;
-      r[j + 1] = (r[j + 1] - a1) * 256.0;
-      const __nv_bfloat162 h = __floats2bfloat162_rn((float)a0 * scale, (float)a1 * scale);
-      packed[j / 2] = *reinterpret_cast<const uint32_t *>(&h);
+      const float v0 = __int_as_float((int)f0[j]) - 8388736.0f;  // 2^23 + 128
+      const float v1 = __int_as_float((int)f0[j + 1]) - 8388736.0f;
+      packed[j / 2] = __byte_perm(__float_as_uint(v0), __float_as_uint(v1), 0x7632);
+    }
+    *reinterpret_cast<uint4 *>(reinterpret_cast<char *>(tiles[0]) + off) =
+        make_uint4(packed[0], packed[1], packed[2], packed[3]);
+  }
+#pragma unroll
+  for (int s = 1; s < SP_SLICES; ++s) {
+    const float sc = __int_as_float((127 - 8 * s) << 23);  // 2^(-8 s)
+    const float bias = -8388736.0f * sc;
+    const uint32_t sel = 0x7540u + (uint32_t)(4 - s);     // byte 4 - s of lp, then 0x00, 0x00, 0x4B
+    uint32_t packed[4];
+#pragma unroll
+    for (int j = 0; j < 8; j += 2) {
+      const float v0 = fmaf(__uint_as_float(__byte_perm(lo[j], 0x4B000000u, sel)), sc, bias);
+      const float v1 = fmaf(__uint_as_float(__byte_perm(lo[j + 1], 0x4B000000u, sel)), sc, bias);
+      packed[j / 2] = __byte_perm(__float_as_uint(v0), __float_as_uint(v1), 0x7632);
     }
     *reinterpret_cast<uint4 *>(reinterpret_cast<char *>(tiles[s]) + off) =
         make_uint4(packed[0], packed[1], packed[2], packed[3]);
   }
 }
 
-// 2^e >= |m| with e from frexp (e = 0 for m = 0); returns {2^(e-7), 2^-e}.
-__device__ __forceinline__ void pow2_scale(double m, double *scale, double *inv) {
+// 2^e >= |m| with e from frexp (e = 0 for m = 0, e >= -960 so that the
+// fixed-point factor stays finite); returns {2^(e - 7), 2^(39 - e)}.
+__device__ __forceinline__ void pow2_scale(double m, double *scale, double *sc39) {
   int e = 0;
   if (m > 0.0) frexp(m, &e);
+  e = max(e, -960);
   *scale = ldexp(1.0, e - 7);
-  *inv = ldexp(1.0, -e);
+  *sc39 = ldexp(1.0, 39 - e);
 }
 
 struct SplitParams {
@@ -352,10 +381,7 @@ __device__ void producer_role(const SplitParams &P, SplitSmem &S, int ptid, int 
       const int koff = 8 * kseg;
 #pragma unroll
       for (int h = 0; h < 2; ++h) {
-        double y[8];
-#pragma unroll
-        for (int j = 0; j < 8; ++j) y[j] = R.a[h][j] * invA[h];
-        split8_store(y, S.A[stage], tile_off(rows[h], koff));
+        split8_store(R.a[h], invA[h], S.A[stage], tile_off(rows[h], koff));
       }
       const bool more = st + 1 < n_stages;
       if (more) {
@@ -366,10 +392,7 @@ __device__ void producer_role(const SplitParams &P, SplitSmem &S, int ptid, int 
       // B half
 #pragma unroll
       for (int h = 0; h < 2; ++h) {
-        double y[8];
-#pragma unroll
-        for (int j = 0; j < 8; ++j) y[j] = R.b[h][j] * invB[h];
-        split8_store(y, S.B[stage], tile_off(rows[h], koff));
+        split8_store(R.b[h], invB[h], S.B[stage], tile_off(rows[h], koff));
       }
       fence_proxy_async_smem();
       __syncwarp();
