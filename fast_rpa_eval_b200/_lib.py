@@ -25,6 +25,13 @@ FRPA_ERR_OOM = 4
 FRPA_ERR_UNSUPPORTED = 5
 RHO1_FP64 = 0
 RHO1_SPLIT_BF16 = 1
+# frpa_rho1_plan_set_tuning keys
+TUNE_FP64_TILE_POINTS = 1
+TUNE_FP64_CTAS_PER_SM = 2
+TUNE_SPLIT_TILE_POINTS = 3
+TUNE_ORDER = 4
+TUNINGS = {"fp64_tile_points": TUNE_FP64_TILE_POINTS, "fp64_ctas_per_sm": TUNE_FP64_CTAS_PER_SM,
+           "split_tile_points": TUNE_SPLIT_TILE_POINTS, "order": TUNE_ORDER}
 
 c_int = ctypes.c_int
 c_ll = ctypes.c_longlong
@@ -162,7 +169,16 @@ def _ptr(t):
 
 
 def _stream(stream):
+    """cudaStream_t for a torch stream, an integer handle, or None (torch's
+    current stream, so that calls inside a CUDA-graph capture are captured)."""
     if stream is None:
+        try:
+            import torch
+
+            if torch.cuda.is_available() and torch.cuda.is_initialized():
+                return c_void_p(torch.cuda.current_stream().cuda_stream)
+        except ImportError:
+            pass
         return c_void_p(0)
     if hasattr(stream, "cuda_stream"):
         return c_void_p(stream.cuda_stream)
@@ -195,6 +211,20 @@ class Rho1Plan:
         f = c_int(0)
         check(lib().frpa_rho1_device_flags(self.handle, ctypes.byref(f)))
         return f.value
+
+    def set_tuning(self, **kw):
+        """fp64_tile_points (64 | 128), fp64_ctas_per_sm (0..2),
+        split_tile_points (16..128), order (0 largest first | 1 batch order)."""
+        for k, v in kw.items():
+            check(lib().frpa_rho1_plan_set_tuning(self.handle, c_int(TUNINGS[k]), c_int(int(v))))
+
+    def tuning(self) -> dict:
+        out = {}
+        for k, key in TUNINGS.items():
+            v = c_int(0)
+            check(lib().frpa_rho1_plan_get_tuning(self.handle, c_int(key), ctypes.byref(v)))
+            out[k] = v.value
+        return out
 
     def adjoint_p1(self, n_active, wave, gwave, g_rho, g_grad, dP1, stream=None):
         check(lib().frpa_rho1_adjoint_p1(self.handle, c_int(n_active), _ptr(wave), _ptr(gwave), _ptr(g_rho),
@@ -456,3 +486,23 @@ def probe_fp64_tflops(kind: str = "mma") -> float:
     fn = lib().frpa_probe_fp64_mma_tflops if kind == "mma" else lib().frpa_probe_fp64_fma_tflops
     check(fn(ctypes.byref(v), c_void_p(0)))
     return v.value
+
+
+def capture_graph(fn, warmup: int = 1):
+    """A torch.cuda.CUDAGraph of ``fn()`` (plan launches on the current stream:
+    the library allocates nothing after plan creation, so its launches
+    capture).  ``fn`` runs ``warmup`` times first, outside the capture, so
+    that one-time kernel attribute set-up happens before it.  Replay with
+    ``graph.replay()``."""
+    import torch
+
+    side = torch.cuda.Stream()
+    side.wait_stream(torch.cuda.current_stream())
+    with torch.cuda.stream(side):
+        for _ in range(warmup):
+            fn()
+    torch.cuda.current_stream().wait_stream(side)
+    g = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(g):
+        fn()
+    return g

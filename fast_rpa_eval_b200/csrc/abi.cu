@@ -86,7 +86,7 @@ static int rho1_plan_build(Rho1Plan **out, const frpa_rho1_desc *D) {
                              D->i_basis_batches && D->i_batch_2_wave_offset),
                  "rho1: null array argument");
   const long long wave_len = D->wave_alloc_len > 0 ? D->wave_alloc_len : (nb > 0 ? D->i_batch_2_wave_offset[nb] : 0);
-  std::vector<Rho1WorkItem> items;
+  std::vector<Rho1WorkItem> items, batches;
   std::vector<int> ibc;
   std::vector<int> ib_off(nb, 0);
   long long map_len = 0, n_valid_pts = 0;
@@ -120,12 +120,7 @@ static int rho1_plan_build(Rho1Plan **out, const frpa_rho1_desc *D) {
     nc_max = std::max(nc_max, nc);
     ++n_valid_b;
     n_valid_pts += np;
-    if (np == 0) continue;
-    const int tiles = (np + 63) / 64;
-    int w = (np + tiles - 1) / tiles;
-    w = std::min(64, (w + 7) & ~7);
-    for (int p0 = 0; p0 < np; p0 += w)
-      items.push_back(Rho1WorkItem{b, nc, np, p0, std::min(w, np - p0), ib_off[b], pre, 0, off});
+    batches.push_back(Rho1WorkItem{b, nc, np, 0, np, ib_off[b], pre, 0, off});
   }
   for (long long i = 0; i < map_len; ++i)
     FRPA_CHECK_ARG(D->i_valid_point_2_i_full_points_map[i] >= 0 &&
@@ -133,9 +128,7 @@ static int rho1_plan_build(Rho1Plan **out, const frpa_rho1_desc *D) {
                    "rho1: i_valid_point_2_i_full_points_map[%lld] = %d outside 0..%d", i,
                    D->i_valid_point_2_i_full_points_map[i], D->n_full_points - 1);
   // largest first: the persistent kernel takes items in this order
-  std::stable_sort(items.begin(), items.end(), [](const Rho1WorkItem &a, const Rho1WorkItem &b) {
-    return (long long)a.nc * a.nc * a.pn > (long long)b.nc * b.nc * b.pn;
-  });
+  rho1_fp64_build_items(batches, 64, 0, &items);
 
   Rho1Plan *P = new Rho1Plan();
   FRPA_CUDA_TRY(cudaGetDevice(&P->device));
@@ -161,11 +154,10 @@ static int rho1_plan_build(Rho1Plan **out, const frpa_rho1_desc *D) {
       st = fail(FRPA_ERR_CUDA, "rho1: plan upload failed");
   };
   up((void **)&P->d_items, items.data(), sizeof(Rho1WorkItem) * items.size());
+  P->h_batches = batches;
   {
     std::vector<Rho1WorkItem> split;
-    std::vector<int> npb(nb);
-    for (int b = 0; b < nb; ++b) npb[b] = D->n_point_batches[b];
-    rho1_split_build_items(items, npb.data(), nb, &split);
+    rho1_split_build_items(batches, P->split_tile_points, P->order, &split);
     P->n_items_split = (int)split.size();
     up((void **)&P->d_items_split, split.data(), sizeof(Rho1WorkItem) * split.size());
     std::vector<double> zeros((size_t)D->n_basis * T, 0.0);
@@ -439,6 +431,64 @@ int frpa_rho1_device_flags(const frpa_rho1_plan *plan, int *flags) {
   FRPA_CUDA_TRY(cudaMemcpy(flags, plan->p->d_err, sizeof(int), cudaMemcpyDeviceToHost));
   FRPA_CUDA_TRY(cudaMemset(plan->p->d_err, 0, sizeof(int)));
   return FRPA_OK;
+}
+
+// Re-uploads a work list (synchronous; not inside a stream capture).
+static int replace_items(Rho1WorkItem **dst, int *count, const std::vector<Rho1WorkItem> &items) {
+  Rho1WorkItem *d = nullptr;
+  FRPA_CUDA_TRY(cudaMalloc(&d, sizeof(Rho1WorkItem) * std::max<size_t>(items.size(), 1)));
+  if (!items.empty() &&
+      cudaMemcpy(d, items.data(), sizeof(Rho1WorkItem) * items.size(), cudaMemcpyHostToDevice) != cudaSuccess) {
+    cudaFree(d);
+    return fail(FRPA_ERR_CUDA, "rho1: work-list upload failed");
+  }
+  cudaFree(*dst);
+  *dst = d;
+  *count = (int)items.size();
+  return FRPA_OK;
+}
+
+int frpa_rho1_plan_set_tuning(frpa_rho1_plan *plan, int key, int value) {
+  if (!plan) return fail(FRPA_ERR_INVALID, "rho1: null plan");
+  Rho1Plan &P = *plan->p;
+  switch (key) {
+    case FRPA_TUNE_FP64_TILE_POINTS:
+      FRPA_CHECK_ARG(value == 64 || value == 128, "rho1 tuning: FP64 tile points %d not 64 or 128", value);
+      P.fp64_tile_points = value;
+      break;
+    case FRPA_TUNE_FP64_CTAS_PER_SM:
+      FRPA_CHECK_ARG(value >= 0 && value <= 2, "rho1 tuning: CTAs per SM %d not 0..2", value);
+      P.fp64_ctas_per_sm = value;
+      return FRPA_OK;
+    case FRPA_TUNE_SPLIT_TILE_POINTS:
+      FRPA_CHECK_ARG(value >= 16 && value <= 128, "rho1 tuning: split tile points %d not 16..128", value);
+      P.split_tile_points = value;
+      break;
+    case FRPA_TUNE_ORDER:
+      FRPA_CHECK_ARG(value == 0 || value == 1, "rho1 tuning: order %d not 0 or 1", value);
+      P.order = value;
+      break;
+    default:
+      return fail(FRPA_ERR_INVALID, "rho1 tuning: unknown key %d", key);
+  }
+  std::vector<Rho1WorkItem> items, split;
+  rho1_fp64_build_items(P.h_batches, P.fp64_tile_points, P.order, &items);
+  rho1_split_build_items(P.h_batches, P.split_tile_points, P.order, &split);
+  FRPA_TRY(replace_items(&P.d_items, &P.n_items, items));
+  FRPA_TRY(replace_items(&P.d_items_split, &P.n_items_split, split));
+  return FRPA_OK;
+}
+
+int frpa_rho1_plan_get_tuning(const frpa_rho1_plan *plan, int key, int *value) {
+  if (!plan || !value) return fail(FRPA_ERR_INVALID, "rho1: null argument");
+  const Rho1Plan &P = *plan->p;
+  switch (key) {
+    case FRPA_TUNE_FP64_TILE_POINTS: *value = P.fp64_tile_points; return FRPA_OK;
+    case FRPA_TUNE_FP64_CTAS_PER_SM: *value = P.fp64_ctas_per_sm; return FRPA_OK;
+    case FRPA_TUNE_SPLIT_TILE_POINTS: *value = P.split_tile_points; return FRPA_OK;
+    case FRPA_TUNE_ORDER: *value = P.order; return FRPA_OK;
+    default: return fail(FRPA_ERR_INVALID, "rho1 tuning: unknown key %d", key);
+  }
 }
 
 int frpa_rho1_adjoint_p1(const frpa_rho1_plan *plan, int n_active, const double *wave, const double *gradient_wave,

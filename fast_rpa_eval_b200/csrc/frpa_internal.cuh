@@ -124,7 +124,18 @@ struct Rho1Plan {
   int n_items_split = 0;
   double *d_rowmax = nullptr;
   int *d_err = nullptr;
+  // tunings (frpa_rho1_plan_set_tuning) and the host copy of the valid
+  // batches the work lists are rebuilt from (one item per batch, p0 = 0)
+  int fp64_tile_points = 64;   // 64 or 128 points per FP64 work item
+  int fp64_ctas_per_sm = 0;    // 0: as many as fit
+  int split_tile_points = 128; // <= 128 points per split-BF16 work item
+  int order = 0;               // 0: largest items first, 1: batch order
+  std::vector<Rho1WorkItem> h_batches;
 };
+
+// Work lists of a plan's valid batches (one entry per batch in `batches`).
+void rho1_fp64_build_items(const std::vector<Rho1WorkItem> &batches, int tile_points, int order,
+                           std::vector<Rho1WorkItem> *out);
 
 int rho1_fp64_launch(const Rho1Plan &plan, int n_active, const double *wave, const double *gwave,
                      const double *P1, const double *bias, const double *gbias, double *rho, double *grad,
@@ -133,7 +144,7 @@ int rho1_fp64_grid(int device);
 int rho1_split_launch(const Rho1Plan &plan, int n_active, const double *wave, const double *gwave,
                       const double *P1, const double *bias, const double *gbias, double *rho, double *grad,
                       cudaStream_t stream);
-void rho1_split_build_items(const std::vector<Rho1WorkItem> &fp64_items, const int *np_b, int n_batches,
+void rho1_split_build_items(const std::vector<Rho1WorkItem> &batches, int tile_points, int order,
                             std::vector<Rho1WorkItem> *out);
 
 int rho1_adjoint_launch_items(const Rho1Plan &plan, const void *d_items, int n_items, int n_active,

@@ -16,20 +16,32 @@
 // contracts each finished work1 tile against phi / grad phi, so work1 never
 // leaves the SM.  Per-point sums are reduced in a fixed order (registers ->
 // warp shuffles -> two shared-memory slots), so results are deterministic.
+#include <algorithm>
+#include <vector>
+
 #include "frpa_internal.cuh"
 
 namespace frpa {
 namespace {
 
 constexpr int BM = 64;       // rows (i_compute) per tile
-constexpr int BN = 64;       // points per tile
 constexpr int KC = 16;       // contraction chunk
 constexpr int STAGES = 3;    // cp.async pipeline depth
-constexpr int THREADS = 256; // 8 warps: 2 along M x 4 along N, warp tile 32 x 16
 constexpr int LDA = BM + 4;  // As[k][m]: stride = 4 (mod 16) doubles -> conflict-free fragment loads
 constexpr int LDB = KC + 4;  // Bs[n][k]
 constexpr int MAX_NC = FRPA_MAX_N_COMPUTE;
 
+// Tile shapes: BN points per work item, 2 warps along M x BN / 16 along N,
+// warp tile 32 x 16.  BN = 64: 256 threads, 2 CTAs per SM; BN = 128: 512
+// threads, one CTA per SM, each gathered P1c tile serving twice the points.
+template <int BN>
+struct Fp64Shape {
+  static constexpr int WN = BN / 16;
+  static constexpr int THREADS = 64 * WN;
+  static constexpr int MIN_BLOCKS = BN == 64 ? 2 : 1;
+};
+
+template <int BN>
 struct Smem {
   double A[STAGES][KC * LDA];
   double B[STAGES][BN * LDB];
@@ -38,18 +50,20 @@ struct Smem {
   int next;
 };
 
-__global__ void __launch_bounds__(THREADS, 2)
+template <int BN>
+__global__ void __launch_bounds__(Fp64Shape<BN>::THREADS, Fp64Shape<BN>::MIN_BLOCKS)
     rho1_fp64_kernel(const Rho1WorkItem *__restrict__ items, int n_items, int *__restrict__ counter,
                      const int *__restrict__ ib_all, const int *__restrict__ map, int T, int n_active, int n_basis,
                      int n_full_points, int n_max_batch_size, int n_batches, const double *__restrict__ wave,
                      const double *__restrict__ gwave, const double *__restrict__ P1,
                      const double *__restrict__ bias, const double *__restrict__ gbias, double *__restrict__ rho,
                      double *__restrict__ grad, int aligned16) {
+  constexpr int THREADS = Fp64Shape<BN>::THREADS, WN = Fp64Shape<BN>::WN;
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  Smem &S = *reinterpret_cast<Smem *>(smem_raw);
+  Smem<BN> &S = *reinterpret_cast<Smem<BN> *>(smem_raw);
   const int tid = threadIdx.x;
   const int lane = tid & 31, warp = tid >> 5;
-  const int wm = warp >> 2, wn = warp & 3;
+  const int wm = warp / WN, wn = warp % WN;
   const int g = lane >> 2, q = lane & 3;
   const long long nb2 = (long long)n_basis * n_basis;
 
@@ -238,20 +252,46 @@ __global__ void __launch_bounds__(THREADS, 2)
   }
 }
 
+template <int BN>
+int fp64_grid(int device, int ctas_per_sm) {
+  static int cached[64] = {0};
+  const int smem = (int)sizeof(Smem<BN>);
+  if (device < 0 || device >= 64 || !cached[device]) {
+    if (cudaFuncSetAttribute(rho1_fp64_kernel<BN>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) != cudaSuccess)
+      return 0;
+    int per_sm = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, rho1_fp64_kernel<BN>, Fp64Shape<BN>::THREADS, smem) !=
+        cudaSuccess)
+      return 0;
+    if (device >= 0 && device < 64) cached[device] = per_sm > 0 ? per_sm : 1;
+    if (device < 0 || device >= 64) return 0;
+  }
+  int n_sm = 0;
+  if (cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, device) != cudaSuccess) return 0;
+  const int per_sm = ctas_per_sm > 0 ? std::min(ctas_per_sm, cached[device]) : cached[device];
+  return per_sm * n_sm;
+}
+
+template <int BN>
+int fp64_launch(const Rho1Plan &plan, int n_active, const double *wave, const double *gwave, const double *P1,
+                const double *bias, const double *gbias, double *rho, double *grad, cudaStream_t stream) {
+  int grid = fp64_grid<BN>(plan.device, plan.fp64_ctas_per_sm);
+  if (grid <= 0) return fail(FRPA_ERR_CUDA, "rho1_fp64: occupancy query failed");
+  if (grid > plan.n_items) grid = plan.n_items;
+  rho1_fp64_kernel<BN><<<grid, Fp64Shape<BN>::THREADS, sizeof(Smem<BN>), stream>>>(
+      plan.d_items, plan.n_items, plan.d_counter, plan.d_ib, plan.d_map, plan.T, n_active, plan.n_basis,
+      plan.n_full_points, plan.n_max_batch_size, plan.n_batches, wave, gwave, P1, bias, gbias, rho, grad,
+      plan.wave_aligned16);
+  FRPA_LAUNCH_CHECK();
+  return FRPA_OK;
+}
+
 }  // namespace
 
+// Sets the kernels' shared-memory attributes once per device (outside any
+// stream capture); 0 on failure.
 int rho1_fp64_grid(int device) {
-  static int cached[64] = {0};
-  if (device >= 0 && device < 64 && cached[device]) return cached[device];
-  const int smem = (int)sizeof(Smem);
-  if (cudaFuncSetAttribute(rho1_fp64_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) != cudaSuccess)
-    return 0;
-  int per_sm = 0, n_sm = 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, rho1_fp64_kernel, THREADS, smem) != cudaSuccess) return 0;
-  if (cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, device) != cudaSuccess) return 0;
-  const int grid = (per_sm > 0 ? per_sm : 1) * n_sm;
-  if (device >= 0 && device < 64) cached[device] = grid;
-  return grid;
+  return fp64_grid<64>(device, 0) > 0 && fp64_grid<128>(device, 0) > 0 ? fp64_grid<64>(device, 0) : 0;
 }
 
 int rho1_fp64_launch(const Rho1Plan &plan, int n_active, const double *wave, const double *gwave, const double *P1,
@@ -262,15 +302,29 @@ int rho1_fp64_launch(const Rho1Plan &plan, int n_active, const double *wave, con
       grad, 0, sizeof(double) * 3 * (size_t)plan.n_max_batch_size * plan.n_batches * plan.T, stream));
   if (plan.n_items == 0) return FRPA_OK;
   FRPA_CUDA_TRY(cudaMemsetAsync(plan.d_counter, 0, sizeof(int), stream));
-  int grid = plan.grid_fp64 > 0 ? plan.grid_fp64 : rho1_fp64_grid(plan.device);
-  if (grid <= 0) return fail(FRPA_ERR_CUDA, "rho1_fp64: occupancy query failed");
-  if (grid > plan.n_items) grid = plan.n_items;
-  rho1_fp64_kernel<<<grid, THREADS, sizeof(Smem), stream>>>(
-      plan.d_items, plan.n_items, plan.d_counter, plan.d_ib, plan.d_map, plan.T, n_active, plan.n_basis,
-      plan.n_full_points, plan.n_max_batch_size, plan.n_batches, wave, gwave, P1, bias, gbias, rho, grad,
-      plan.wave_aligned16);
-  FRPA_LAUNCH_CHECK();
-  return FRPA_OK;
+  if (plan.fp64_tile_points == 128)
+    return fp64_launch<128>(plan, n_active, wave, gwave, P1, bias, gbias, rho, grad, stream);
+  return fp64_launch<64>(plan, n_active, wave, gwave, P1, bias, gbias, rho, grad, stream);
+}
+
+// Work items of <= tile_points points (a batch's points split evenly, widths a
+// multiple of 8), largest nc^2 x points first or in batch order.
+void rho1_fp64_build_items(const std::vector<Rho1WorkItem> &batches, int tile_points, int order,
+                           std::vector<Rho1WorkItem> *out) {
+  out->clear();
+  for (const Rho1WorkItem &b : batches) {
+    if (b.np == 0) continue;
+    const int tiles = (b.np + tile_points - 1) / tile_points;
+    int w = (b.np + tiles - 1) / tiles;
+    w = std::min(tile_points, (w + 7) & ~7);
+    for (int p0 = 0; p0 < b.np; p0 += w)
+      out->push_back(Rho1WorkItem{b.batch, b.nc, b.np, p0, std::min(w, b.np - p0), b.ib_off, b.prefix, 0,
+                                  b.wave_off});
+  }
+  if (order == 0)
+    std::stable_sort(out->begin(), out->end(), [](const Rho1WorkItem &a, const Rho1WorkItem &b) {
+      return (long long)a.nc * a.nc * a.pn > (long long)b.nc * b.nc * b.pn;
+    });
 }
 
 }  // namespace frpa

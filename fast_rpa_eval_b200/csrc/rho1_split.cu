@@ -704,24 +704,25 @@ int rho1_split_launch(const Rho1Plan &plan, int n_active, const double *wave, co
   return FRPA_OK;
 }
 
-// Work items of the split path: point tiles of <= 128 points, largest first.
-void rho1_split_build_items(const std::vector<Rho1WorkItem> &fp64_items, const int *np_b, int n_batches,
+// Work items of the split path: point tiles of <= tile_points (<= 128)
+// points, a batch's points split evenly; largest first or in batch order.
+void rho1_split_build_items(const std::vector<Rho1WorkItem> &batches, int tile_points, int order,
                             std::vector<Rho1WorkItem> *out) {
-  (void)n_batches;
   out->clear();
-  std::vector<int> seen;
-  for (const Rho1WorkItem &w : fp64_items) {
-    if (w.p0 != 0) continue;  // one entry per batch
-    const int np = np_b[w.batch];
-    const int tiles = (np + SP_M - 1) / SP_M;
+  const int tp = std::max(1, std::min(tile_points, SP_M));
+  for (const Rho1WorkItem &w : batches) {
+    const int np = w.np;
+    if (np == 0) continue;
+    const int tiles = (np + tp - 1) / tp;
     const int width = (np + tiles - 1) / tiles;
     for (int p0 = 0; p0 < np; p0 += width)
       out->push_back(Rho1WorkItem{w.batch, w.nc, w.np, p0, std::min(width, np - p0), w.ib_off, w.prefix, 0,
                                   w.wave_off});
   }
-  std::stable_sort(out->begin(), out->end(), [](const Rho1WorkItem &a, const Rho1WorkItem &b) {
-    return (long long)a.nc * a.nc * a.pn > (long long)b.nc * b.nc * b.pn;
-  });
+  if (order == 0)
+    std::stable_sort(out->begin(), out->end(), [](const Rho1WorkItem &a, const Rho1WorkItem &b) {
+      return (long long)a.nc * a.nc * a.pn > (long long)b.nc * b.nc * b.pn;
+    });
 }
 
 }  // namespace frpa

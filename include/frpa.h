@@ -213,6 +213,25 @@ int frpa_rho1_execute(const frpa_rho1_plan *plan, int mode, int n_active, const 
                       const double *gradient_wave, const double *P1, const double *bias, const double *gbias,
                       double *rho, double *grad, void *stream);
 
+/* Tunings of a plan's rho1 launches (no counterpart in the reference, whose
+ * MAGMA batching has fixed shapes).  Keys and values:
+ *   FRPA_TUNE_FP64_TILE_POINTS  64 (256 threads, 2 CTAs per SM) or 128 (512
+ *                               threads, 1 CTA per SM: each gathered P1c tile
+ *                               serves twice the points);
+ *   FRPA_TUNE_FP64_CTAS_PER_SM  0 (as many as fit), 1 or 2;
+ *   FRPA_TUNE_SPLIT_TILE_POINTS 16..128 points per split-BF16 work item;
+ *   FRPA_TUNE_ORDER             0 largest items first, 1 batch order.
+ * Results are unchanged by every setting.  Setting rebuilds and re-uploads the
+ * work lists (synchronous: call it outside any stream capture). */
+enum {
+  FRPA_TUNE_FP64_TILE_POINTS = 1,
+  FRPA_TUNE_FP64_CTAS_PER_SM = 2,
+  FRPA_TUNE_SPLIT_TILE_POINTS = 3,
+  FRPA_TUNE_ORDER = 4
+};
+int frpa_rho1_plan_set_tuning(frpa_rho1_plan *plan, int key, int value);
+int frpa_rho1_plan_get_tuning(const frpa_rho1_plan *plan, int key, int *value);
+
 /* Adjoint: dP1 (n_basis, n_basis, T) += d(sum g_rho . rho1 + sum g_grad . grad)/dP1.
  * g_rho (n_full_points, T) or NULL, g_grad like grad or NULL.  dP1 is NOT zeroed. */
 int frpa_rho1_adjoint_p1(const frpa_rho1_plan *plan, int n_active, const double *wave, const double *gradient_wave,
