@@ -492,6 +492,21 @@ def run_frpa(args, ranks: Ranks):
                         "tflops_fp64": achieved_tf, "frac_of_measured_fp64_mma": achieved_tf / fp64_peak,
                         "hbm_gbs_algorithmic": w.bytes / (ms_fp64 / 1e3) / 1e9}
 
+    # the bias producer (generate_first_order_rho_bias_part2) for a 4-atom tile
+    # on the same batches, P1 standing in for the ground-state density matrix
+    av = torch.from_numpy(np.ascontiguousarray(p.atom_valid_n_compute_c_batches.ravel(order="F"),
+                                               dtype=np.int32)).cuda()
+    bias4 = torch.zeros(p.n_max_batch_size * p.n_my_batches_work * 4, dtype=torch.float64, device="cuda")
+    na = min(4, p.n_atoms)
+
+    def bias_step():
+        w.plan.bias_part2(4, p.n_atoms, 1, na, 1, av, w.wave, w.gwave, w.P1, bias4)
+
+    ms_bias = time_device_steps(bias_step, args.steps, args.warmup, ranks, stream)
+    out["bias_part2_4_atoms"] = {"ms_per_call": ms_bias, "pts_per_s": total_pts / (ms_bias / 1e3),
+                                 "device_flags": w.plan.device_flags()}
+    del av, bias4
+
     # end to end through the reference-named session entry point
     e2e = None
     if not args.no_e2e:

@@ -212,6 +212,15 @@ class Rho1Plan:
         check(lib().frpa_rho1_device_flags(self.handle, ctypes.byref(f)))
         return f.value
 
+    def bias_part2(self, T, n_atoms, j_atom_begin, j_atom_end, j_coord, atom_valid, wave, gwave, density_matrix,
+                   out, stream=None):
+        """first_order_rho_bias_part2 (n_max_batch_size, n_batches, T) on the device
+        (generate_first_order_rho_bias_part2.cpp:11-168); atom_valid is the int32
+        (n_atoms + 1, n_batches) array of 0-based compute ranges."""
+        check(lib().frpa_rho1_bias_part2(self.handle, c_int(T), c_int(n_atoms), c_int(j_atom_begin),
+                                         c_int(j_atom_end), c_int(j_coord), _ptr(atom_valid), _ptr(wave),
+                                         _ptr(gwave), _ptr(density_matrix), _ptr(out), _stream(stream)))
+
     def set_tuning(self, **kw):
         """fp64_tile_points (64 | 128), fp64_ctas_per_sm (0..2),
         split_tile_points (16..128), order (0 largest first | 1 batch order)."""
@@ -506,3 +515,32 @@ def capture_graph(fn, warmup: int = 1):
     with torch.cuda.graph(g):
         fn()
     return g
+
+
+def dropin_bias_part2(prob, density_matrix, j_coord: int = 1, bias=None):
+    """generate_first_order_rho_bias_part2_ through the reference-named entry
+    point (host arrays); returns (n_max_batch_size, n_batches, 4)."""
+    L = lib()
+    nmb, nb = prob.n_max_batch_size, prob.n_my_batches_work
+    out = np.zeros(nmb * nb * 4) if bias is None else np.array(bias, dtype=np.float64).ravel(order="F").copy()
+    keep = []
+
+    def ip(a):
+        a = np.ascontiguousarray(np.asarray(a).ravel(order="F"), dtype=np.int32)
+        keep.append(a)
+        return a.ctypes.data_as(c_int_p)
+
+    def dp(a):
+        a = np.ascontiguousarray(np.asarray(a).ravel(order="F"), dtype=np.float64)
+        keep.append(a)
+        return a.ctypes.data_as(c_dbl_p)
+
+    ints = [nb, prob.j_atom_begin, prob.j_atom_end, j_coord, prob.n_full_points, prob.n_basis, prob.n_atoms,
+            prob.n_max_compute_ham, prob.n_centers_basis_I, nmb]
+    refs = [ctypes.byref(c_int(int(v))) for v in ints]
+    L.generate_first_order_rho_bias_part2_(
+        *refs, ip(prob.batch_sizes), ip(prob.n_point_batches), ip(prob.n_compute_c_batches), ip(prob.i_basis_batches),
+        ip(prob.atom_valid_n_compute_c_batches), ip(prob.i_batch_2_wave_offset), dp(prob.wave),
+        dp(prob.gradient_wave), out.ctypes.data_as(c_dbl_p), dp(prob.partition_tab), dp(density_matrix))
+    check_void_call()
+    return out.reshape((nmb, nb, 4), order="F")

@@ -491,6 +491,14 @@ int frpa_rho1_plan_get_tuning(const frpa_rho1_plan *plan, int key, int *value) {
   }
 }
 
+int frpa_rho1_bias_part2(const frpa_rho1_plan *plan, int T, int n_atoms, int j_atom_begin, int j_atom_end,
+                         int j_coord, const int *atom_valid, const double *wave, const double *gradient_wave,
+                         const double *density_matrix, double *first_order_rho_bias_part2, void *stream) {
+  if (!plan) return fail(FRPA_ERR_INVALID, "bias part 2: null plan");
+  return rho1_bias_part2_launch(*plan->p, nullptr, atom_valid, n_atoms, j_atom_begin, j_atom_end, j_coord, T, wave,
+                                gradient_wave, density_matrix, first_order_rho_bias_part2, (cudaStream_t)stream);
+}
+
 int frpa_rho1_adjoint_p1(const frpa_rho1_plan *plan, int n_active, const double *wave, const double *gradient_wave,
                          const double *g_rho, const double *g_grad, double *dP1, void *stream) {
   if (!plan) return fail(FRPA_ERR_INVALID, "rho1: null plan");
@@ -598,6 +606,61 @@ void evaluate_first_order_rho_reduce_memory_c_v3_batches_atoms_(
   if (st == FRPA_OK) {
     cudaError_t e = cudaStreamSynchronize(s);
     if (e != cudaSuccess) fail(FRPA_ERR_CUDA, "rho1: %s", cudaGetErrorString(e));
+  }
+  rho1_plan_free(P);
+}
+
+void generate_first_order_rho_bias_part2_(
+    int *n_my_batches_work, int *j_atom_begin, int *j_atom_end, int *j_coord, int *n_full_points, int *n_basis,
+    int *n_atoms, int *n_max_compute_ham, int *n_centers_basis_I, int *n_max_batch_size, int *batch_sizes,
+    int *n_point_batches, int *n_compute_c_batches, int *i_basis_batches, int *atom_valid_n_compute_c_batches,
+    int *i_batch_2_wave_offset, double *wave_batches_compress, double *gradient_wave_batches_compress,
+    double *first_order_rho_bias_part2, double *partition_tab, double *density_matrix) {
+  (void)n_full_points;
+  (void)n_max_compute_ham;
+  (void)batch_sizes;
+  (void)partition_tab;
+  std::lock_guard<std::mutex> lk(g_buf_mu);
+  clear_error();
+  constexpr int T = 4;  // generate_first_order_rho_bias_part2.cpp:4
+  if (!n_my_batches_work || !n_point_batches || !atom_valid_n_compute_c_batches || !density_matrix ||
+      !first_order_rho_bias_part2) {
+    fail(FRPA_ERR_INVALID, "bias part 2: null argument");
+    return;
+  }
+  const int nb = *n_my_batches_work;
+  // the reference does not use the point map here: a contiguous numbering
+  std::vector<int> pre(nb + 1, 0);
+  for (int b = 0; b < nb; ++b) pre[b + 1] = pre[b] + std::max(0, n_point_batches[b]);
+  std::vector<int> ident(std::max(1, pre[nb]));
+  for (size_t i = 0; i < ident.size(); ++i) ident[i] = (int)i;
+  int n_full = std::max(1, pre[nb]);
+  frpa_rho1_desc d = rho_desc_from_ref(T, n_my_batches_work, &n_full, n_basis, n_centers_basis_I, n_max_batch_size,
+                                       n_point_batches, pre.data(), ident.data(), n_compute_c_batches,
+                                       i_basis_batches, i_batch_2_wave_offset);
+  Rho1Plan *P = nullptr;
+  if (rho1_plan_build(&P, &d) != FRPA_OK) return;
+  const size_t wl = (size_t)P->wave_len, nbias = (size_t)d.n_max_batch_size * nb * T;
+  const size_t nav = (size_t)(*n_atoms + 1) * nb, ndm = (size_t)d.n_basis * d.n_basis;
+  double *w = nullptr, *gw = nullptr, *dm = nullptr, *bi = nullptr;
+  int *av = nullptr;
+  cudaStream_t s = 0;
+  int st = FRPA_OK;
+  if (st == FRPA_OK) st = h2d(16, wave_batches_compress, wl, &w, s);
+  if (st == FRPA_OK) st = h2d(17, gradient_wave_batches_compress, 3 * wl, &gw, s);
+  if (st == FRPA_OK) st = h2d(18, density_matrix, ndm, &dm, s);
+  if (st == FRPA_OK) st = h2d(19, first_order_rho_bias_part2, nbias, &bi, s);
+  if (st == FRPA_OK) st = h2d(20, atom_valid_n_compute_c_batches, nav, &av, s);
+  if (st == FRPA_OK)
+    st = rho1_bias_part2_launch(*P, atom_valid_n_compute_c_batches, av, *n_atoms, *j_atom_begin, *j_atom_end,
+                                *j_coord, T, w, gw, dm, bi, s);
+  if (st == FRPA_OK &&
+      cudaMemcpyAsync(first_order_rho_bias_part2, bi, sizeof(double) * nbias, cudaMemcpyDeviceToHost, s) !=
+          cudaSuccess)
+    st = fail(FRPA_ERR_CUDA, "bias part 2: download failed");
+  if (st == FRPA_OK) {
+    cudaError_t e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) fail(FRPA_ERR_CUDA, "bias part 2: %s", cudaGetErrorString(e));
   }
   rho1_plan_free(P);
 }

@@ -147,6 +147,9 @@ int rho1_split_launch(const Rho1Plan &plan, int n_active, const double *wave, co
 void rho1_split_build_items(const std::vector<Rho1WorkItem> &batches, int tile_points, int order,
                             std::vector<Rho1WorkItem> *out);
 
+int rho1_bias_part2_launch(const Rho1Plan &plan, const int *h_atom_valid, const int *d_atom_valid, int n_atoms,
+                           int j_atom_begin, int j_atom_end, int j_coord, int T, const double *wave,
+                           const double *gwave, const double *dm, double *bias, cudaStream_t stream);
 int rho1_adjoint_launch_items(const Rho1Plan &plan, const void *d_items, int n_items, int n_active,
                               const double *wave, const double *gwave, const double *g_rho, const double *g_grad,
                               double *dP1, cudaStream_t stream);

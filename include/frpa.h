@@ -138,6 +138,21 @@ void sum_up_whole_potential_c_v3_atoms_full_points_j_atom_tile_cu_host_(
     const double *log_r_grid_inc, const double *scale_radial, const double *partition_tab,
     double *delta_v_hartree);
 
+/* Replaces generate_first_order_rho_bias_part2_
+ * (generate_first_order_rho_bias_part2.cpp:11-168): the density-matrix part
+ * of the rho1 bias for atoms j_atom_begin..j_atom_end along j_coord, written
+ * to first_order_rho_bias_part2 (n_max_batch_size, n_batches, 4) -- the
+ * reference fixes this array's atom tile at 4 (:4).  Batches without compute
+ * functions are left as they were; n_full_points, n_max_compute_ham,
+ * batch_sizes and partition_tab are accepted and unused, as in the reference.
+ * At most 64 compute functions of one atom per batch. */
+void generate_first_order_rho_bias_part2_(
+    int *n_my_batches_work, int *j_atom_begin, int *j_atom_end, int *j_coord, int *n_full_points, int *n_basis,
+    int *n_atoms, int *n_max_compute_ham, int *n_centers_basis_I, int *n_max_batch_size, int *batch_sizes,
+    int *n_point_batches, int *n_compute_c_batches, int *i_basis_batches, int *atom_valid_n_compute_c_batches,
+    int *i_batch_2_wave_offset, double *wave_batches_compress, double *gradient_wave_batches_compress,
+    double *first_order_rho_bias_part2, double *partition_tab, double *density_matrix);
+
 /* Replaces init_dfpt_device_info (device.hpp:191, device.cu:7-33): selects
  * device 0 (or $FRPA_DEVICE) and creates the session stream. */
 void init_dfpt_device_info(void);
@@ -212,6 +227,17 @@ int frpa_rho1_plan_info(const frpa_rho1_plan *plan, long long *info3);
 int frpa_rho1_execute(const frpa_rho1_plan *plan, int mode, int n_active, const double *wave,
                       const double *gradient_wave, const double *P1, const double *bias, const double *gbias,
                       double *rho, double *grad, void *stream);
+
+/* The same bias on the device with a plan's work list: atom_valid
+ * ((n_atoms + 1, n_batches), 0-based ranges as in the reference), wave,
+ * gradient_wave, density_matrix (n_basis, n_basis) and the output
+ * (n_max_batch_size, n_batches, T) are device pointers; atoms
+ * j_atom_begin..j_atom_end (at most T of them, 1-based).  Ranges that leave a
+ * batch's compute functions (or exceed 64 per atom) are skipped and set bit 3
+ * of frpa_rho1_device_flags. */
+int frpa_rho1_bias_part2(const frpa_rho1_plan *plan, int T, int n_atoms, int j_atom_begin, int j_atom_end,
+                         int j_coord, const int *atom_valid, const double *wave, const double *gradient_wave,
+                         const double *density_matrix, double *first_order_rho_bias_part2, void *stream);
 
 /* Tunings of a plan's rho1 launches (no counterpart in the reference, whose
  * MAGMA batching has fixed shapes).  Keys and values:

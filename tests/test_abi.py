@@ -25,6 +25,7 @@ def test_header_declares_the_reference_entry_points():
                 "evaluate_first_order_rho_reduce_memory_c_v3_batches_atoms_cu_host_",
                 "sum_up_whole_potential_c_v3_atoms_full_points_j_atom_tile_",
                 "sum_up_whole_potential_c_v3_atoms_full_points_j_atom_tile_cu_host_",
+                "generate_first_order_rho_bias_part2_",
                 "init_dfpt_device_info", "init_dfpt_device_data", "free_dfpt_device_data", "free_dfpt_device_info"):
         assert ref in names
 

@@ -1,0 +1,83 @@
+"""The bias producer (generate_first_order_rho_bias_part2) on the GPU against
+the oracle: plan entry point and reference-named drop-in, every j_coord,
+symmetric and non-symmetric density matrices, NaN wave padding.  Stated
+tolerance: 1e-12 normwise relative (FP64; the two reference GEMM terms are
+summed as one contraction, so rounding differs)."""
+
+import numpy as np
+import pytest
+
+import oracle
+from fast_rpa_eval_b200 import _lib, synth
+
+TOL = 1e-12
+
+
+def rel(a, b):
+    return float(np.max(np.abs(a - b)) / max(np.max(np.abs(b)), 1e-300))
+
+
+def _problem(seed=4):
+    p = synth.make_rho1_problem(T=4, seed=seed, n_atoms=6, n_batches=24, pad_value=np.nan, n_active=3)
+    p.j_atom_begin, p.j_atom_end = 2, 4
+    return p
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("j_coord", [1, 3])
+@pytest.mark.parametrize("symmetric", [True, False])
+def test_bias_plan_matches_oracle(j_coord, symmetric):
+    import torch
+
+    from gpu_util import dev, host
+
+    p = _problem()
+    dm = np.random.default_rng(2).normal(size=(p.n_basis, p.n_basis))
+    if symmetric:
+        dm = dm + dm.T
+    ref = oracle.rho_bias_part2(p, dm, j_coord=j_coord)
+    plan = _lib.Rho1Plan(p)
+    out = torch.zeros(p.n_max_batch_size * p.n_my_batches_work * 4, dtype=torch.float64, device="cuda")
+    av = dev(p.atom_valid_n_compute_c_batches, np.int32)
+    plan.bias_part2(4, p.n_atoms, p.j_atom_begin, p.j_atom_end, j_coord, av, dev(p.wave), dev(p.gradient_wave),
+                    dev(dm), out)
+    torch.cuda.synchronize()
+    got = host(out, (p.n_max_batch_size, p.n_my_batches_work, 4))
+    assert rel(got[:, :, :3], ref[:, :, :3]) < TOL
+    assert np.all(got[:, :, 3] == 0.0)
+    assert plan.device_flags() == 0
+
+
+@pytest.mark.gpu
+def test_bias_dropin_matches_reference_entry_semantics():
+    p = _problem(seed=7)
+    dm = np.random.default_rng(5).normal(size=(p.n_basis, p.n_basis))
+    init = np.full((p.n_max_batch_size, p.n_my_batches_work, 4), 9.0)
+    got = _lib.dropin_bias_part2(p, dm, j_coord=2, bias=init)
+    ref = oracle.rho_bias_part2(p, dm, j_coord=2)
+    # written: points of batches with compute functions, atoms j_atom_begin..j_atom_end;
+    # everything else keeps the caller's values, as in the reference
+    written = np.zeros(got.shape, dtype=bool)
+    for b in range(p.n_my_batches_work):
+        if p.n_compute_c_batches[b] > 0:
+            written[: p.n_point_batches[b], b, :3] = True
+    assert rel(np.where(written, got, 0.0), np.where(written, ref, 0.0)) < TOL
+    assert np.all(got[~written] == 9.0)
+
+
+@pytest.mark.gpu
+def test_bias_flags_a_range_outside_the_batch():
+    import torch
+
+    from gpu_util import dev
+
+    p = _problem()
+    av = np.array(p.atom_valid_n_compute_c_batches, dtype=np.int32, order="F").copy()
+    b = int(np.argmax(p.n_compute_c_batches))
+    av[p.j_atom_begin, b] = p.n_compute_c_batches[b] + 5  # atom j_atom_begin's range leaves batch b
+    plan = _lib.Rho1Plan(p)
+    out = torch.zeros(p.n_max_batch_size * p.n_my_batches_work * 4, dtype=torch.float64, device="cuda")
+    plan.bias_part2(4, p.n_atoms, p.j_atom_begin, p.j_atom_end, 1, dev(av, np.int32), dev(p.wave),
+                    dev(p.gradient_wave), dev(np.eye(p.n_basis)), out)
+    torch.cuda.synchronize()
+    assert plan.device_flags() & 8
