@@ -52,6 +52,9 @@ def parse_args():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=10.0, help="target CPU-baseline sample time")
     ap.add_argument("--no-tune", action="store_true", help="skip the autotuner (default tile shapes)")
+    ap.add_argument("--config4-sizes", default="2000",
+                    help="config-4 sweep sizes in atoms (comma list; 2000,10000,40000 for the full sweep)")
+    ap.add_argument("--no-config4", action="store_true", help="skip the config-4 sweep")
     ap.add_argument("--mode", choices=["fp64", "split"], default=None,
                     help="headline rho1 path (default: split if built, else fp64)")
     return ap.parse_args()
@@ -458,6 +461,8 @@ def run_frpa(args, ranks: Ranks):
     graphs = {m: _lib.capture_graph(lambda m=m: w.step(m, None))
               for m in (_lib.RHO1_FP64, _lib.RHO1_SPLIT_BF16)}
 
+    n_items_tuned = w.plan.info()["n_items"]
+
     # both rho1 paths are timed on the same inputs; the headline is --mode
     clocks = ClockSampler(ranks.local)
     clocks.start()
@@ -569,6 +574,16 @@ def run_frpa(args, ranks: Ranks):
             del sp
     out["sumup_config3"] = sumup
 
+    # config 4: the config-1 recipe swept to thousands of atoms (chunked, one
+    # graph-captured autotuned launch per chunk and path)
+    if not args.no_config4:
+        from fast_rpa_eval_b200 import sweep
+
+        del w
+        torch.cuda.empty_cache()
+        out["config4_sweep"] = [sweep.run_sweep(int(n), seed=4 + 7919 * ranks.rank, tune=not args.no_tune)
+                                for n in args.config4_sizes.split(",") if n.strip()]
+
     if mode == _lib.RHO1_FP64:
         roofline = {"bound": "tensor", "achieved": achieved_tf, "peak": fp64_peak, "unit": "TFLOP/s",
                     "frac": achieved_tf / fp64_peak, "traffic": profile_traffic("rho1_fp64_kernel"),
@@ -592,7 +607,7 @@ def run_frpa(args, ranks: Ranks):
         "data": "synthetic (seeded config-2 recipe: Gaussian x Y_lm basis, phi generated on the GPU)",
         "config": {"workload": "config2: rho1 + grad rho1, 1000 atoms at 0.1/A^3, 10 functions/atom, "
                                f"{p.n_my_batches_work} batches of 100-300 points, n_compute 100-600, T=1",
-                   "path": mode_name, "valid_batches": info["n_valid_batches"], "work_items": w.plan.info()["n_items"],
+                   "path": mode_name, "valid_batches": info["n_valid_batches"], "work_items": n_items_tuned,
                    "launch": "one persistent grouped launch per step, replayed from a CUDA graph",
                    "tuning": tuned or "defaults (--no-tune)",
                    "grid_points_per_rank": w_points,

@@ -302,6 +302,13 @@ def synth_basis_values(prob, points_dev, wave_dev, gwave_dev, pad_value=0.0, str
                                         ctypes.c_double(pad_value), _ptr(wave_dev), _ptr(gwave_dev), _stream(stream)))
 
 
+def synth_p1_window(global_index, n: int, T: int, scale: float, seed: int, out, stream=None):
+    """Device window (n, n, T) of a symmetric synthetic P1 keyed by global basis
+    indices (frpa_synth_p1_window); global_index: int32 device tensor."""
+    check(lib().frpa_synth_p1_window(_ptr(global_index), c_int(n), c_int(T), ctypes.c_double(scale),
+                                     ctypes.c_ulonglong(seed), _ptr(out), _stream(stream)))
+
+
 def set_atom_tile_size(T: int):
     check(lib().frpa_set_atom_tile_size(c_int(T)))
 

@@ -555,6 +555,11 @@ int frpa_synth_basis_values(const frpa_rho1_desc *desc, const double *points, in
                             gradient_wave, (cudaStream_t)stream);
 }
 
+int frpa_synth_p1_window(const int *global_index, int n, int T, double scale, unsigned long long seed, double *out,
+                         void *stream) {
+  return synth_p1_window(global_index, n, T, scale, seed, out, (cudaStream_t)stream);
+}
+
 // ------------------------------------------------- reference drop-ins
 
 void evaluate_first_order_rho_reduce_memory_c_v3_batches_atoms_(

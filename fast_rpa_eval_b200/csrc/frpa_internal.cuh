@@ -147,6 +147,8 @@ int rho1_split_launch(const Rho1Plan &plan, int n_active, const double *wave, co
 void rho1_split_build_items(const std::vector<Rho1WorkItem> &batches, int tile_points, int order,
                             std::vector<Rho1WorkItem> *out);
 
+int synth_p1_window(const int *gidx, int n, int T, double scale, unsigned long long seed, double *out,
+                    cudaStream_t stream);
 int rho1_bias_part2_launch(const Rho1Plan &plan, const int *h_atom_valid, const int *d_atom_valid, int n_atoms,
                            int j_atom_begin, int j_atom_end, int j_coord, int T, const double *wave,
                            const double *gwave, const double *dm, double *bias, cudaStream_t stream);

@@ -217,4 +217,48 @@ int synth_basis_values(const frpa_rho1_desc *D, const double *points, int n_atom
   return st;
 }
 
+namespace {
+
+// splitmix64 finaliser: a counter-based hash of the entry's coordinates.
+__device__ __forceinline__ unsigned long long mix64(unsigned long long z) {
+  z += 0x9E3779B97F4A7C15ull;
+  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+  z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+  return z ^ (z >> 31);
+}
+
+// out(i, j, t) = scale N(0,1)-like draw keyed by (seed, t, min(g_i, g_j),
+// max(g_i, g_j)) with g the window's global basis indices: a symmetric P1
+// whose entries do not depend on the window they are evaluated in
+// (Box-Muller on two 53-bit uniforms from the hash).
+__global__ void synth_p1_window_kernel(const int *__restrict__ gidx, int n, int T, double scale,
+                                       unsigned long long seed, double *__restrict__ out) {
+  const long long nn = (long long)n * n;
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < nn * T;
+       e += (long long)gridDim.x * blockDim.x) {
+    const long long t = e / nn, r = e - t * nn;
+    const int i = (int)(r % n), j = (int)(r / n);
+    const unsigned long long a = (unsigned long long)min(gidx[i], gidx[j]);
+    const unsigned long long b = (unsigned long long)max(gidx[i], gidx[j]);
+    const unsigned long long h1 = mix64(seed ^ mix64(a * 0x100000001B3ull + b) ^ mix64((unsigned long long)t + 7));
+    const unsigned long long h2 = mix64(h1 ^ 0xD1B54A32D192ED03ull);
+    const double u1 = ((h1 >> 11) + 1) * 0x1.0p-53;  // (0, 1]
+    const double u2 = (h2 >> 11) * 0x1.0p-53;
+    out[e] = scale * sqrt(-2.0 * log(u1)) * cospi(2.0 * u2);
+  }
+}
+
+}  // namespace
+
+int synth_p1_window(const int *gidx, int n, int T, double scale, unsigned long long seed, double *out,
+                    cudaStream_t stream) {
+  FRPA_CHECK_ARG(gidx && out && n >= 0 && T >= 1, "synth P1 window: bad argument");
+  if (n == 0) return FRPA_OK;
+  const long long total = (long long)n * n * T;
+  const int grid = (int)std::min<long long>((total + 255) / 256, 148 * 32);
+  synth_p1_window_kernel<<<grid, 256, 0, stream>>>(gidx, n, T, scale, seed, out);
+  if (cudaGetLastError() != cudaSuccess) return fail(FRPA_ERR_CUDA, "synth P1 window: launch failed");
+  return FRPA_OK;
+}
+
 }  // namespace frpa

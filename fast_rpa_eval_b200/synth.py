@@ -627,3 +627,143 @@ def host_basis_values(prob: Rho1Problem, n_batches: int | None = None, pad_value
         wave[off[b]:off[b] + ncp * npb].reshape(npb, ncp)[:, :nc] = phi.T
         gwave[3 * off[b]:3 * off[b] + 3 * ncp * npb].reshape(npb, 3, ncp)[:, :, :nc] = np.transpose(gphi, (2, 1, 0))
     return wave, gwave
+
+
+# --------------------------------------------------------------------------
+# Config 4: the config-1 recipe swept to thousands of atoms
+# --------------------------------------------------------------------------
+
+
+@dataclass
+class SweepGeometry:
+    """Atoms, basis and batches of a config-4 sweep.  Batches are ordered so
+    that consecutive ones sit near each other (6 A cells), which keeps the
+    basis window of a chunk of batches small."""
+
+    atoms: np.ndarray  # (n_atoms, 3)
+    basis: Basis
+    centre: np.ndarray  # centre atom of each batch
+    npts: np.ndarray
+    ncs: np.ndarray
+    ib: list  # selected functions (global, sorted) per batch
+    seed: int
+    point_radius: float = 3.0
+
+    @property
+    def n_batches(self) -> int:
+        return int(len(self.centre))
+
+
+def config4_geometry(n_atoms: int, seed: int = 4, batches_per_atom: int = 8, np_range=(50, 400),
+                     nc_range=(50, 800), density: float = 8 / 216.0, shells: str = "sssspdd") -> SweepGeometry:
+    """Config 4: the config-1 recipe (20 functions per atom: 4 s + 2 p + 2 d,
+    Gaussian radials, density of config 1) at ``n_atoms`` atoms, 8 batches per
+    atom, points per batch and n_compute log-uniform over 50-400 and 50-800
+    (n_compute chosen as the strongest functions by radial envelope over the
+    batch ball among the nearest atoms)."""
+    from scipy.spatial import cKDTree
+
+    rng = np.random.default_rng(seed)
+    atoms = place_atoms(n_atoms, rng, density=density, min_dist=1.0)
+    basis = make_basis(n_atoms, shells, rng)
+    fpa = basis.n // n_atoms
+    centre = np.repeat(np.arange(n_atoms), batches_per_atom)
+    cell = np.floor(atoms[centre] / 6.0).astype(np.int64)
+    centre = centre[np.lexsort((cell[:, 2], cell[:, 1], cell[:, 0]))]
+    nb = len(centre)
+
+    def logu(lo, hi):
+        return np.floor(np.exp(rng.uniform(np.log(lo), np.log(hi + 1), nb))).astype(np.int64).clip(lo, hi)
+
+    npts, ncs = logu(*np_range), logu(*nc_range)
+    k_near = int(min(n_atoms, 2 * int(ncs.max()) // fpa + 8))
+    tree = cKDTree(atoms)
+    ib = [None] * nb
+    funcs_of_atom = np.arange(basis.n).reshape(n_atoms, fpa)
+    radius = 3.0
+    for b0 in range(0, nb, 4096):
+        b1 = min(nb, b0 + 4096)
+        d_near, near = tree.query(atoms[centre[b0:b1]], k=k_near)
+        for k, b in enumerate(range(b0, b1)):
+            cand = funcs_of_atom[near[k]].ravel()
+            d = np.repeat(d_near[k], fpa)
+            lo, hi = np.maximum(d - radius, 0.0), d + radius
+            lv = basis.l[cand].astype(np.float64)
+            al = basis.alpha[cand]
+            rstar = np.clip(np.sqrt(lv / (2 * al)), lo, hi)
+            score = rstar**lv * np.exp(-al * rstar * rstar)
+            nc = int(min(ncs[b], len(cand)))
+            ncs[b] = nc
+            ib[b] = np.sort(cand[np.argpartition(-score, nc - 1)[:nc]])
+    return SweepGeometry(atoms=atoms, basis=basis, centre=centre, npts=npts, ncs=ncs, ib=ib, seed=seed,
+                         point_radius=radius)
+
+
+def sweep_chunks(geom: SweepGeometry, max_batches: int = 5000, max_window: int = 24000):
+    """Consecutive batch ranges [b0, b1) whose basis window (union of their
+    compute functions) has at most max_window functions."""
+    chunks, b0 = [], 0
+    nb = geom.n_batches
+    while b0 < nb:
+        seen = set()
+        b1 = b0
+        while b1 < nb and b1 - b0 < max_batches:
+            new = seen.union(geom.ib[b1].tolist())
+            if len(new) > max_window and b1 > b0:
+                break
+            seen = new
+            b1 += 1
+        chunks.append((b0, b1))
+        b0 = b1
+    return chunks
+
+
+def sweep_chunk_problem(geom: SweepGeometry, b0: int, b1: int) -> tuple[Rho1Problem, np.ndarray]:
+    """Batches [b0, b1) of a sweep as a standalone rho1 problem over its basis
+    window U (returned as the global 0-based indices of the window's
+    functions): points drawn per batch from a generator keyed by (seed, b0),
+    phi / grad phi left to the device generator, P1 left to
+    frpa_synth_p1_window over U, biases zero, T = 1."""
+    ids = np.arange(b0, b1)
+    U = np.unique(np.concatenate([geom.ib[b] for b in ids]))
+    atoms_u = np.unique(geom.basis.atom[U])
+    basis_u = Basis(np.searchsorted(atoms_u, geom.basis.atom[U]).astype(np.int32), geom.basis.l[U],
+                    geom.basis.m[U], geom.basis.alpha[U])
+    rng = np.random.default_rng([geom.seed, b0])
+    npts = geom.npts[ids].astype(np.int64)
+    ncs = geom.ncs[ids].astype(np.int64)
+    tot = int(npts.sum())
+    u = rng.normal(size=(tot, 3))
+    u /= np.linalg.norm(u, axis=1, keepdims=True)
+    r = geom.point_radius * rng.uniform(0, 1, tot) ** (1.0 / 3.0)
+    owner = np.repeat(np.arange(len(ids)), npts)
+    pts = geom.atoms[geom.centre[ids][owner]] + u * r[:, None]
+    nb = len(ids)
+    nmc = int(max(1, ncs.max()))
+    i_basis = np.zeros((nmc, nb), np.int32, order="F")
+    avn = np.zeros((len(atoms_u) + 1, nb), np.int32, order="F")
+    for k, b in enumerate(ids):
+        loc = np.searchsorted(U, geom.ib[b])
+        i_basis[: len(loc), k] = loc + 1
+        avn[1:, k] = np.cumsum(np.bincount(basis_u.atom[loc], minlength=len(atoms_u)))
+    prefix = np.zeros(nb + 1, np.int32)
+    prefix[1:] = np.cumsum(npts)
+    ncp = ((ncs + 3) // 4) * 4
+    off = np.zeros(nb + 1, np.int64)
+    off[1:] = np.cumsum(ncp * npts)
+    if off[-1] >= 2**31:
+        raise ValueError("chunk too large for int32 wave offsets")
+    nmb = int(npts.max())
+    prob = Rho1Problem(
+        T=1, j_atom_begin=1, j_atom_end=1, j_coord=1, n_my_batches_work=nb, n_full_points=max(1, tot),
+        n_basis=len(U), n_atoms=len(atoms_u), n_max_compute_ham=nmc, n_centers_basis_I=nmc, n_max_batch_size=nmb,
+        batch_sizes=npts.astype(np.int32), n_point_batches=npts.astype(np.int32), n_point_batches_prefix_sum=prefix,
+        i_valid_point_2_i_full_points_map=np.arange(max(1, tot), dtype=np.int32),
+        n_compute_c_batches=ncs.astype(np.int32), i_basis_batches=i_basis, atom_valid_n_compute_c_batches=avn,
+        i_batch_2_wave_offset=off.astype(np.int32), wave=None, gradient_wave=None,
+        first_order_density_matrix=np.zeros((1, 1, 1), order="F"),
+        first_order_rho_bias_part2=np.zeros((nmb, nb, 1), order="F"),
+        first_order_gradient_rho_bias=np.zeros((3, nmb, nb, 1), order="F"),
+        basis_atom=(basis_u.atom + 1).astype(np.int32), partition_tab=np.ones(max(1, tot)), density_matrix=None,
+        atoms_xyz=geom.atoms[atoms_u], basis=basis_u, valid_points_xyz=pts)
+    return prob, U.astype(np.int32)

@@ -351,6 +351,14 @@ int frpa_synth_basis_values(const frpa_rho1_desc *desc, const double *points, in
                             const int *basis_atom, const int *basis_l, const int *basis_m, const double *basis_alpha,
                             double pad_value, double *wave, double *gradient_wave, void *stream);
 
+/* Synthetic workloads: a window of a symmetric first-order density matrix
+ * out (n, n, T) (device) whose entry (i, j, t) is scale x a standard-normal
+ * draw keyed by (seed, t, the pair of global basis indices global_index[i],
+ * global_index[j]) -- the same global P1 whichever window it is evaluated in,
+ * for sweeps whose full P1 would not fit (global_index: device, n entries). */
+int frpa_synth_p1_window(const int *global_index, int n, int T, double scale, unsigned long long seed, double *out,
+                         void *stream);
+
 /* Measured FP64 tensor-pipe throughput of the current device (independent
  * m8n8k4 f64 MMAs on every SM), the ceiling the plain FP64 rho1 contraction
  * is compared against.  Takes a few tens of milliseconds. */
