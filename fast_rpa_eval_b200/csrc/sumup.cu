@@ -78,6 +78,7 @@ struct SumupPlan {
   int n_coef = 0, rs = 0;
   // device const arrays
   int *d_map = nullptr;
+  int *d_order = nullptr;  // valid points in spatial (Morton) order, for warp-uniform branches
   double *d_coord = nullptr;
   int *d_species = nullptr, *d_species_center = nullptr, *d_l_hartree = nullptr, *d_n_grid = nullptr;
   int *d_c2a = nullptr, *d_chp = nullptr, *d_icc = nullptr, *d_ncc = nullptr, *d_ijkmax = nullptr;
@@ -235,10 +236,10 @@ __device__ double near_field(int lam, int L2, double dx, double dy, double dz, d
 // --------------------------------------------------------- fast kernel ---
 
 __global__ void __launch_bounds__(SU_THREADS)
-    sumup_fast_kernel(int n_valid, int n_full, const int *__restrict__ map, const double *__restrict__ coord,
-                      int n_active, int n_chp, int n_atoms, int L, int n_hartree_grid,
-                      const double *__restrict__ recs, const double *__restrict__ spline, double *__restrict__ dv,
-                      unsigned char *__restrict__ codes) {
+    sumup_fast_kernel(int n_valid, int n_full, const int *__restrict__ map, const int *__restrict__ order,
+                      const double *__restrict__ coord, int n_active, int n_chp, int n_atoms, int L,
+                      int n_hartree_grid, const double *__restrict__ recs, const double *__restrict__ spline,
+                      double *__restrict__ dv, unsigned char *__restrict__ codes) {
   const int RS = rec_stride(L);
   const int CO = rec_coef_off(L);
   const int L2 = (L + 1) * (L + 1);
@@ -251,8 +252,11 @@ __global__ void __launch_bounds__(SU_THREADS)
   bool valid[SU_PPT];
 #pragma unroll
   for (int j = 0; j < SU_PPT; ++j) {
-    vidx[j] = blockIdx.x * (SU_THREADS * SU_PPT) + j * SU_THREADS + tid;
-    valid[j] = vidx[j] < n_valid;
+    // a warp's points are neighbours in space when the plan gives an order,
+    // so its near / far / skip decisions for an atom mostly agree
+    const int slot = blockIdx.x * (SU_THREADS * SU_PPT) + j * SU_THREADS + tid;
+    valid[j] = slot < n_valid;
+    vidx[j] = valid[j] ? (order ? order[slot] : slot) : 0;
     full[j] = valid[j] ? map[vidx[j]] : 0;
     px[j] = valid[j] ? coord[3LL * full[j] + 0] : 0.0;
     py[j] = valid[j] ? coord[3LL * full[j] + 1] : 0.0;
@@ -427,7 +431,8 @@ int launch_fast(const SumupPlan &P, int n_active, const double *spline, double *
                 cudaStream_t stream) {
   const int per_block = SU_THREADS * SU_PPT;
   const int grid = (P.n_valid_points + per_block - 1) / per_block;
-  sumup_fast_kernel<<<grid, SU_THREADS, 0, stream>>>(P.n_valid_points, P.n_full_points, P.d_map, P.d_coord,
+  sumup_fast_kernel<<<grid, SU_THREADS, 0, stream>>>(P.n_valid_points, P.n_full_points, P.d_map, P.d_order,
+                                                     P.d_coord,
                                                      n_active, P.n_chp, P.n_atoms, P.L, P.n_hartree_grid, P.d_recs,
                                                      spline, dv, codes);
   FRPA_LAUNCH_CHECK();
@@ -608,7 +613,7 @@ int sumup_upload_constants(int device) {
 
 void sumup_plan_free(SumupPlan *P) {
   if (!P) return;
-  void *ptrs[] = {P->d_map, P->d_coord, P->d_species, P->d_species_center, P->d_l_hartree, P->d_n_grid,
+  void *ptrs[] = {P->d_map, P->d_order, P->d_coord, P->d_species, P->d_species_center, P->d_l_hartree, P->d_n_grid,
                   P->d_c2a, P->d_chp, P->d_icc, P->d_ncc, P->d_ijkmax, P->d_icc_packed, P->d_cc, P->d_cc_xyz,
                   P->d_rgm, P->d_linc, P->d_conv_ptr, P->d_conv_n, P->d_conv_f, P->d_mc, P->d_recs, P->d_err,
                   P->d_convT_ptr, P->d_convT_k, P->d_convT_f, P->d_dcoef, P->d_dmc};
@@ -757,6 +762,43 @@ int sumup_plan_create(SumupPlan **out, const frpa_sumup_desc *D) {
 #define UP(field, src, bytes) \
   if (st == FRPA_OK) st = upload((void **)&P->field, (src), (bytes));
   UP(d_map, D->i_valid_point_2_i_full_points_map, sizeof(int) * (size_t)D->n_valid_points);
+  {
+    // Morton order of the valid points (21 bits per axis over their bounding box)
+    const int nv = D->n_valid_points;
+    std::vector<int> ord(nv);
+    if (nv > 0) {
+      double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
+      for (int i = 0; i < nv; ++i)
+        for (int c = 0; c < 3; ++c) {
+          const double x = D->coord_points[3LL * D->i_valid_point_2_i_full_points_map[i] + c];
+          lo[c] = std::min(lo[c], x);
+          hi[c] = std::max(hi[c], x);
+        }
+      auto spread = [](uint64_t v) {
+        v &= 0x1fffff;
+        v = (v | v << 32) & 0x1f00000000ffffull;
+        v = (v | v << 16) & 0x1f0000ff0000ffull;
+        v = (v | v << 8) & 0x100f00f00f00f00full;
+        v = (v | v << 4) & 0x10c30c30c30c30c3ull;
+        v = (v | v << 2) & 0x1249249249249249ull;
+        return v;
+      };
+      std::vector<std::pair<uint64_t, int>> key(nv);
+      for (int i = 0; i < nv; ++i) {
+        uint64_t k = 0;
+        for (int c = 0; c < 3; ++c) {
+          const double x = D->coord_points[3LL * D->i_valid_point_2_i_full_points_map[i] + c];
+          const double w = hi[c] > lo[c] ? (x - lo[c]) / (hi[c] - lo[c]) : 0.0;
+          const uint64_t q = (uint64_t)std::min(2097151.0, std::max(0.0, w * 2097151.0));
+          k |= spread(q) << c;
+        }
+        key[i] = {k, i};
+      }
+      std::sort(key.begin(), key.end());
+      for (int i = 0; i < nv; ++i) ord[i] = key[i].second;
+    }
+    UP(d_order, ord.data(), sizeof(int) * (size_t)nv);
+  }
   UP(d_coord, D->coord_points, sizeof(double) * 3 * (size_t)D->n_full_points);
   UP(d_species, D->species, sizeof(int) * D->n_atoms);
   UP(d_species_center, D->species_center, sizeof(int) * D->n_centers);
