@@ -99,6 +99,17 @@ def main():
         lines.append("  }")
         lines.append("}")
         lines.append("")
+    lines.append("// kelvin_eval<N>: N points at a time")
+    lines.append("template <int N>")
+    lines.append("__device__ __forceinline__ void kelvin_eval(int lam, const double *__restrict__ c, const double *ux, "
+                 "const double *uy, const double *uz, double *P);")
+    for npts in (1, 2):
+        lines.append("template <>")
+        lines.append(f"__device__ __forceinline__ void kelvin_eval<{npts}>(int lam, const double *__restrict__ c, "
+                     "const double *ux, const double *uy, const double *uz, double *P) {")
+        lines.append(f"  kelvin_eval_{npts}(lam, c, ux, uy, uz, P);")
+        lines.append("}")
+    lines.append("")
     lines.append("}  // namespace frpa")
     lines.append("")
     dst = os.path.join(os.path.dirname(os.path.abspath(__file__)), "kelvin_horner.cuh")

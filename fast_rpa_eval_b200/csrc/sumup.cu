@@ -301,8 +301,11 @@ __global__ void __launch_bounds__(SU_THREADS)
         }
 
         // far field
-        const bool all_far_same = __all_sync(FULL, br[0] == 2 && br[SU_PPT - 1] == 2 && lam[0] == lam[SU_PPT - 1]) &&
-                                  (__reduce_min_sync(FULL, lam[0]) == __reduce_max_sync(FULL, lam[0]));
+        bool mine = true;
+#pragma unroll
+        for (int j = 0; j < SU_PPT; ++j) mine = mine && br[j] == 2 && lam[j] == lam[0];
+        const bool all_far_same =
+            __all_sync(FULL, mine) && (__reduce_min_sync(FULL, lam[0]) == __reduce_max_sync(FULL, lam[0]));
         if (all_far_same) {
           double ux[SU_PPT], uy[SU_PPT], uz[SU_PPT], P[SU_PPT], rinv[SU_PPT];
 #pragma unroll
@@ -313,7 +316,7 @@ __global__ void __launch_bounds__(SU_THREADS)
             uy[j] = dy[j] * ir2;
             uz[j] = dz[j] * ir2;
           }
-          kelvin_eval_2(lam[0], rec + CO, ux, uy, uz, P);
+          kelvin_eval<SU_PPT>(lam[0], rec + CO, ux, uy, uz, P);
 #pragma unroll
           for (int j = 0; j < SU_PPT; ++j) v[j] += P[j] * rinv[j];
         } else {
