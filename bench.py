@@ -579,7 +579,7 @@ def run_frpa(args, ranks: Ranks):
     if not args.no_config4:
         from fast_rpa_eval_b200 import sweep
 
-        del w
+        w = None  # (the sum-up section may have released it already)
         torch.cuda.empty_cache()
         out["config4_sweep"] = [sweep.run_sweep(int(n), seed=4 + 7919 * ranks.rank, tune=not args.no_tune)
                                 for n in args.config4_sizes.split(",") if n.strip()]
