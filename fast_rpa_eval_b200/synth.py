@@ -220,7 +220,7 @@ class Rho1Problem:
 
 def make_rho1_problem(
     n_atoms: int = 8,
-    shells: str = "sssspdd",
+    shells: str = "ssssppdd",
     box: float | None = 6.0,
     density: float | None = None,
     n_batches: int = 64,
@@ -655,7 +655,7 @@ class SweepGeometry:
 
 
 def config4_geometry(n_atoms: int, seed: int = 4, batches_per_atom: int = 8, np_range=(50, 400),
-                     nc_range=(50, 800), density: float = 8 / 216.0, shells: str = "sssspdd") -> SweepGeometry:
+                     nc_range=(50, 800), density: float = 8 / 216.0, shells: str = "ssssppdd") -> SweepGeometry:
     """Config 4: the config-1 recipe (20 functions per atom: 4 s + 2 p + 2 d,
     Gaussian radials, density of config 1) at ``n_atoms`` atoms, 8 batches per
     atom, points per batch and n_compute log-uniform over 50-400 and 50-800

@@ -44,7 +44,7 @@ def test_rho1_fp64_matches_reference_cpu_code():
 
 def test_rho1_uneven_large_batches():
     # n_compute up to 800 and 400 points: many M tiles, uneven point tiles
-    p = synth.make_rho1_problem(T=1, seed=9, n_atoms=60, shells="sssspdd", box=None, density=0.1, n_batches=40,
+    p = synth.make_rho1_problem(T=1, seed=9, n_atoms=60, shells="ssssppdd", box=None, density=0.1, n_batches=40,
                                 np_range=(50, 400), nc_range=(50, 800), log_uniform=True, with_bias=True,
                                 exact_selection=False, pad_value=np.nan)
     r, g = rho1_device_run(_lib.Rho1Plan(p), p)
