@@ -222,7 +222,7 @@ class Rho1Plan:
                                          _ptr(gwave), _ptr(density_matrix), _ptr(out), _stream(stream)))
 
     def set_tuning(self, **kw):
-        """fp64_tile_points (64 | 128), fp64_ctas_per_sm (0..2),
+        """fp64_tile_points (64 | 128), fp64_ctas_per_sm (0..3),
         split_tile_points (16..128), order (0 largest first | 1 batch order)."""
         for k, v in kw.items():
             check(lib().frpa_rho1_plan_set_tuning(self.handle, c_int(TUNINGS[k]), c_int(int(v))))

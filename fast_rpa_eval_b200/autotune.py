@@ -22,7 +22,7 @@ from . import _lib
 
 FP64_SPACE = [
     {"fp64_tile_points": 64, "fp64_ctas_per_sm": 0, "order": 0},
-    {"fp64_tile_points": 64, "fp64_ctas_per_sm": 1, "order": 0},
+    {"fp64_tile_points": 64, "fp64_ctas_per_sm": 2, "order": 0},
     {"fp64_tile_points": 64, "fp64_ctas_per_sm": 0, "order": 1},
     {"fp64_tile_points": 128, "fp64_ctas_per_sm": 0, "order": 0},
     {"fp64_tile_points": 128, "fp64_ctas_per_sm": 0, "order": 1},

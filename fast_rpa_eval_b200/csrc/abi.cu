@@ -457,7 +457,7 @@ int frpa_rho1_plan_set_tuning(frpa_rho1_plan *plan, int key, int value) {
       P.fp64_tile_points = value;
       break;
     case FRPA_TUNE_FP64_CTAS_PER_SM:
-      FRPA_CHECK_ARG(value >= 0 && value <= 2, "rho1 tuning: CTAs per SM %d not 0..2", value);
+      FRPA_CHECK_ARG(value >= 0 && value <= 3, "rho1 tuning: CTAs per SM %d not 0..3", value);
       P.fp64_ctas_per_sm = value;
       return FRPA_OK;
     case FRPA_TUNE_SPLIT_TILE_POINTS:

@@ -25,20 +25,22 @@ namespace frpa {
 namespace {
 
 constexpr int BM = 64;       // rows (i_compute) per tile
-constexpr int KC = 32;       // contraction chunk (32: half the barriers of 16, measured 6% faster)
+constexpr int KC = 16;       // contraction chunk
 constexpr int STAGES = 2;    // cp.async pipeline depth (double buffering)
 constexpr int LDA = BM + 4;  // As[k][m]: stride = 4 (mod 16) doubles -> conflict-free fragment loads
 constexpr int LDB = KC + 4;  // Bs[n][k]
 constexpr int MAX_NC = FRPA_MAX_N_COMPUTE;
 
 // Tile shapes: BN points per work item, 2 warps along M x BN / 16 along N,
-// warp tile 32 x 16.  BN = 64: 256 threads, 2 CTAs per SM; BN = 128: 512
-// threads, one CTA per SM, each gathered P1c tile serving twice the points.
+// warp tile 32 x 16.  BN = 64: 256 threads, 3 CTAs per SM (80 registers,
+// 50 KB of shared memory each; measured faster than 2 CTAs with deeper
+// rings); BN = 128: 512 threads, one CTA per SM, each gathered P1c tile
+// serving twice the points.
 template <int BN>
 struct Fp64Shape {
   static constexpr int WN = BN / 16;
   static constexpr int THREADS = 64 * WN;
-  static constexpr int MIN_BLOCKS = BN == 64 ? 2 : 1;
+  static constexpr int MIN_BLOCKS = BN == 64 ? 3 : 1;
 };
 
 template <int BN>

@@ -241,10 +241,10 @@ int frpa_rho1_bias_part2(const frpa_rho1_plan *plan, int T, int n_atoms, int j_a
 
 /* Tunings of a plan's rho1 launches (no counterpart in the reference, whose
  * MAGMA batching has fixed shapes).  Keys and values:
- *   FRPA_TUNE_FP64_TILE_POINTS  64 (256 threads, 2 CTAs per SM) or 128 (512
- *                               threads, 1 CTA per SM: each gathered P1c tile
- *                               serves twice the points);
- *   FRPA_TUNE_FP64_CTAS_PER_SM  0 (as many as fit), 1 or 2;
+ *   FRPA_TUNE_FP64_TILE_POINTS  64 (256 threads, up to 3 CTAs per SM) or 128
+ *                               (512 threads, 1 CTA per SM: each gathered P1c
+ *                               tile serves twice the points);
+ *   FRPA_TUNE_FP64_CTAS_PER_SM  0 (as many as fit), 1, 2 or 3;
  *   FRPA_TUNE_SPLIT_TILE_POINTS 16..128 points per split-BF16 work item;
  *   FRPA_TUNE_ORDER             0 largest items first, 1 batch order.
  * Results are unchanged by every setting.  Setting rebuilds and re-uploads the
