@@ -25,13 +25,16 @@ FRPA_ERR_OOM = 4
 FRPA_ERR_UNSUPPORTED = 5
 RHO1_FP64 = 0
 RHO1_SPLIT_BF16 = 1
+RHO1_SPLIT_I8 = 2
 # frpa_rho1_plan_set_tuning keys
 TUNE_FP64_TILE_POINTS = 1
 TUNE_FP64_CTAS_PER_SM = 2
 TUNE_SPLIT_TILE_POINTS = 3
 TUNE_ORDER = 4
+TUNE_SPLIT_I8_SCRATCH_MB = 5
 TUNINGS = {"fp64_tile_points": TUNE_FP64_TILE_POINTS, "fp64_ctas_per_sm": TUNE_FP64_CTAS_PER_SM,
-           "split_tile_points": TUNE_SPLIT_TILE_POINTS, "order": TUNE_ORDER}
+           "split_tile_points": TUNE_SPLIT_TILE_POINTS, "order": TUNE_ORDER,
+           "split_i8_scratch_mb": TUNE_SPLIT_I8_SCRATCH_MB}
 
 c_int = ctypes.c_int
 c_ll = ctypes.c_longlong
@@ -223,7 +226,8 @@ class Rho1Plan:
 
     def set_tuning(self, **kw):
         """fp64_tile_points (64 | 128), fp64_ctas_per_sm (0..3),
-        split_tile_points (16..128), order (0 largest first | 1 batch order)."""
+        split_tile_points (16..128), order (0 largest first | 1 batch order),
+        split_i8_scratch_mb (>= 1: packed-operand scratch per group of batches)."""
         for k, v in kw.items():
             check(lib().frpa_rho1_plan_set_tuning(self.handle, c_int(TUNINGS[k]), c_int(int(v))))
 

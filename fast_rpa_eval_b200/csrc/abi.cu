@@ -69,6 +69,7 @@ static void rho1_plan_free(Rho1Plan *P) {
   cudaFree(P->d_items_split);
   cudaFree(P->d_rowmax);
   cudaFree(P->d_err);
+  rho1_i8_free(P);
   delete P;
 }
 
@@ -165,6 +166,7 @@ static int rho1_plan_build(Rho1Plan **out, const frpa_rho1_desc *D) {
     const int z = 0;
     up((void **)&P->d_err, &z, sizeof(int));
   }
+  if (st == FRPA_OK) st = rho1_i8_build(P);
   up((void **)&P->d_ib, ibc.data(), sizeof(int) * ibc.size());
   up((void **)&P->d_map, D->i_valid_point_2_i_full_points_map, sizeof(int) * (size_t)map_len);
   const int zero = 0;
@@ -195,7 +197,7 @@ static int rho1_plan_build(Rho1Plan **out, const frpa_rho1_desc *D) {
   return FRPA_OK;
 }
 
-static int rho1_run(const Rho1Plan &P, int mode, int n_active, const double *wave, const double *gwave,
+static int rho1_run(Rho1Plan &P, int mode, int n_active, const double *wave, const double *gwave,
                     const double *P1, const double *bias, const double *gbias, double *rho, double *grad,
                     cudaStream_t stream) {
   FRPA_CHECK_ARG(P1 && bias && gbias && rho && grad, "rho1: null device pointer");
@@ -206,6 +208,7 @@ static int rho1_run(const Rho1Plan &P, int mode, int n_active, const double *wav
   if (((uintptr_t)wave | (uintptr_t)gwave) & 15) Q.wave_aligned16 = 0;
   if (mode == FRPA_RHO1_FP64) return rho1_fp64_launch(Q, n_active, wave, gwave, P1, bias, gbias, rho, grad, stream);
   if (mode == FRPA_RHO1_SPLIT_BF16) return rho1_split_launch(Q, n_active, wave, gwave, P1, bias, gbias, rho, grad, stream);
+  if (mode == FRPA_RHO1_SPLIT_I8) return rho1_i8_launch(P, n_active, wave, gwave, P1, bias, gbias, rho, grad, stream);
   return fail(FRPA_ERR_INVALID, "rho1: unknown mode %d", mode);
 }
 
@@ -381,7 +384,8 @@ int frpa_set_atom_tile_size(int T) {
 }
 int frpa_get_atom_tile_size(void) { return g_tile; }
 int frpa_set_rho1_mode(int mode) {
-  if (mode != FRPA_RHO1_FP64 && mode != FRPA_RHO1_SPLIT_BF16) return fail(FRPA_ERR_INVALID, "rho1 mode %d", mode);
+  if (mode != FRPA_RHO1_FP64 && mode != FRPA_RHO1_SPLIT_BF16 && mode != FRPA_RHO1_SPLIT_I8)
+    return fail(FRPA_ERR_INVALID, "rho1 mode %d", mode);
   g_rho1_mode = mode;
   return FRPA_OK;
 }
@@ -468,6 +472,11 @@ int frpa_rho1_plan_set_tuning(frpa_rho1_plan *plan, int key, int value) {
       FRPA_CHECK_ARG(value == 0 || value == 1, "rho1 tuning: order %d not 0 or 1", value);
       P.order = value;
       break;
+    case FRPA_TUNE_SPLIT_I8_SCRATCH_MB:
+      FRPA_CHECK_ARG(value >= 1, "rho1 tuning: split-int8 scratch %d MiB not >= 1", value);
+      P.i8_budget = (long long)value << 20;
+      rho1_i8_free(&P);  // groups change: new lists, scratch reallocated by the next execution
+      return rho1_i8_build(&P);
     default:
       return fail(FRPA_ERR_INVALID, "rho1 tuning: unknown key %d", key);
   }
@@ -487,6 +496,7 @@ int frpa_rho1_plan_get_tuning(const frpa_rho1_plan *plan, int key, int *value) {
     case FRPA_TUNE_FP64_CTAS_PER_SM: *value = P.fp64_ctas_per_sm; return FRPA_OK;
     case FRPA_TUNE_SPLIT_TILE_POINTS: *value = P.split_tile_points; return FRPA_OK;
     case FRPA_TUNE_ORDER: *value = P.order; return FRPA_OK;
+    case FRPA_TUNE_SPLIT_I8_SCRATCH_MB: *value = (int)(P.i8_budget >> 20); return FRPA_OK;
     default: return fail(FRPA_ERR_INVALID, "rho1 tuning: unknown key %d", key);
   }
 }

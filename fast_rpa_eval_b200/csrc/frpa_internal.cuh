@@ -97,6 +97,40 @@ struct Rho1WorkItem {
 };
 static_assert(sizeof(Rho1WorkItem) == 40, "work item layout");
 
+// Split-int8 rho1 (rho1_split_i8.cu).  A work item is a point tile of one
+// batch; its phi digits live in the A scratch, the batch's P1c digits (per
+// perturbation) in the B scratch.  Offsets are relative to the scratch of
+// the item's group: groups of consecutive batches are packed and contracted
+// in turn, so the scratch holds one group at a time.
+struct I8Item {
+  int batch, nc, p0, pn;
+  int prefix, rows8, n_nt, n_kc;  // rows8 = pn rounded up to 8; N tiles of <= 96 rows; K chunks of 32
+  long long wave_off;
+  long long a_off;       // bytes of the item's first A chunk
+  long long b_off;       // bytes of the batch's first B chunk (t = 0)
+  long long b_tstride;   // B bytes per perturbation
+  int sa_off;            // first per-point scale of the item
+  int sb_off;            // first per-row scale of the batch (t = 0)
+  int sb_tstride;        // per-row scales per perturbation (n_nt * 96)
+  int pad_;
+};
+static_assert(sizeof(I8Item) == 80, "I8Item layout");
+
+// One N tile of one batch and perturbation, packed by one CTA.
+struct I8BTile {
+  int ib_off, nc, jn, t;
+  int n_rows, n_kc, sb_off, pad_;  // rows of this tile (multiple of 16, <= 96)
+  long long b_off;                 // bytes of the tile's first chunk
+};
+static_assert(sizeof(I8BTile) == 40, "I8BTile layout");
+
+struct I8Group {
+  int item0, item1;   // items [item0, item1)
+  int tile0, tile1;   // B tiles [tile0, tile1)
+  long long a_bytes, b_bytes;
+  int sa_len, sb_len;
+};
+
 struct Rho1Plan {
   int device = 0;
   int T = 1;
@@ -131,6 +165,14 @@ struct Rho1Plan {
   int split_tile_points = 128; // <= 128 points per split-BF16 work item
   int order = 0;               // 0: largest items first, 1: batch order
   std::vector<Rho1WorkItem> h_batches;
+  // split-int8 path: work lists (built with the plan) and the scratch
+  // (allocated by the first split-int8 execution, reused afterwards)
+  I8Item *d_i8_items = nullptr;
+  I8BTile *d_i8_tiles = nullptr;
+  std::vector<I8Group> i8_groups;
+  long long i8_budget = 4LL << 30;  // bytes of A + B scratch per group
+  unsigned char *d_i8_a = nullptr, *d_i8_b = nullptr;
+  double *d_i8_sa = nullptr, *d_i8_sb = nullptr;
 };
 
 // Work lists of a plan's valid batches (one entry per batch in `batches`).
@@ -146,6 +188,12 @@ int rho1_split_launch(const Rho1Plan &plan, int n_active, const double *wave, co
                       cudaStream_t stream);
 void rho1_split_build_items(const std::vector<Rho1WorkItem> &batches, int tile_points, int order,
                             std::vector<Rho1WorkItem> *out);
+
+int p1_rowmax_launch(const Rho1Plan &plan, const double *P1, cudaStream_t stream);
+int rho1_i8_build(Rho1Plan *plan);  // work lists and groups from plan->h_batches
+void rho1_i8_free(Rho1Plan *plan);
+int rho1_i8_launch(Rho1Plan &plan, int n_active, const double *wave, const double *gwave, const double *P1,
+                   const double *bias, const double *gbias, double *rho, double *grad, cudaStream_t stream);
 
 int synth_p1_window(const int *gidx, int n, int T, double scale, unsigned long long seed, double *out,
                     cudaStream_t stream);

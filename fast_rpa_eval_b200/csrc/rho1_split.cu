@@ -45,6 +45,7 @@
 #include <vector>
 
 #include "frpa_internal.cuh"
+#include "sm100_sync.cuh"
 
 namespace frpa {
 namespace {
@@ -64,7 +65,6 @@ constexpr int SP_MAX_K = 1024;    // exactness bound of the FP32 levels 0 and 1
 constexpr int SP_TILE_ELEMS = SP_M * SP_KC;           // one slice tile (bf16 elements)
 constexpr uint32_t SP_LBO = 128;                      // bytes between K-adjacent core matrices
 constexpr uint32_t SP_SBO = (SP_KC / 8) * 128;        // bytes between 8-row groups
-constexpr unsigned long long SP_WAIT_NS = 2000000000ull;  // 2 s per wait
 
 static_assert(SP_M == 128 && SP_N == 128, "instruction shape");
 
@@ -91,84 +91,20 @@ struct SplitSmem {
 
 // ---------------------------------------------------------------- PTX glue
 
-__device__ __forceinline__ uint32_t smem_u32(const void *p) {
-  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
-}
+using sm100::fence_proxy_async_smem;
+using sm100::global_ns;
+using sm100::mbar_arrive;
+using sm100::mbar_init;
+using sm100::mbar_try_wait;
+using sm100::mbar_wait;
+using sm100::smem_u32;
+using sm100::tc_fence_after;
+using sm100::tc_fence_before;
+using sm100::tmem_wait_ld;
+using sm100::umma_commit;
+using sm100::warp_wait;
 
-__device__ __forceinline__ unsigned long long global_ns() {
-  unsigned long long t;
-  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
-  return t;
-}
-
-__device__ __forceinline__ void mbar_init(unsigned long long *bar, uint32_t count) {
-  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count));
-}
-
-__device__ __forceinline__ void mbar_arrive(unsigned long long *bar) {
-  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
-}
-
-__device__ __forceinline__ bool mbar_try_wait(unsigned long long *bar, uint32_t parity) {
-  uint32_t ok;
-  asm volatile(
-      "{\n\t.reg .pred p;\n\t"
-      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-      "selp.u32 %0, 1, 0, p;\n\t}"
-      : "=r"(ok)
-      : "r"(smem_u32(bar)), "r"(parity)
-      : "memory");
-  return ok != 0;
-}
-
-// Bounded wait: false (and the error flag set) if the phase does not
-// complete within SP_WAIT_NS or another role has already given up.
-__device__ __forceinline__ bool mbar_wait(unsigned long long *bar, uint32_t parity, volatile int *abort_flag,
-                                          int *err) {
-  if (mbar_try_wait(bar, parity)) return true;
-  const unsigned long long t0 = global_ns();
-  for (;;) {
-    if (mbar_try_wait(bar, parity)) return true;
-    if (*abort_flag) return false;
-    if (global_ns() - t0 > SP_WAIT_NS) {
-      *abort_flag = 1;
-      atomicOr(err, 2);
-      return false;
-    }
-  }
-}
-
-// Warp-uniform bounded wait: lane 0 polls, the outcome goes to every lane,
-// so a warp never splits over a timeout; __syncwarp orders the lanes' later
-// reads after lane 0's acquire.
-__device__ __forceinline__ bool warp_wait(unsigned long long *bar, uint32_t parity, volatile int *abort_flag,
-                                          int *err, int lane) {
-  int ok = 1;
-  if (lane == 0) ok = mbar_wait(bar, parity, abort_flag, err) ? 1 : 0;
-  ok = __shfl_sync(0xffffffffu, ok, 0);
-  __syncwarp();
-  return ok != 0;
-}
-
-__device__ __forceinline__ void fence_proxy_async_smem() {
-  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-}
-__device__ __forceinline__ void tc_fence_before() {
-  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-}
-__device__ __forceinline__ void tc_fence_after() {
-  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-}
-
-// Shared-memory matrix descriptor: K-major, no swizzle, version 1 (sm_100).
-__device__ __forceinline__ uint64_t smem_desc(uint32_t addr) {
-  uint64_t d = 0;
-  d |= (uint64_t)((addr & 0x3FFFF) >> 4);
-  d |= (uint64_t)(SP_LBO >> 4) << 16;
-  d |= (uint64_t)(SP_SBO >> 4) << 32;
-  d |= (uint64_t)1 << 46;  // version
-  return d;                // base offset 0, lbo mode 0, layout type 0 (no swizzle)
-}
+__device__ __forceinline__ uint64_t smem_desc(uint32_t addr) { return sm100::smem_desc<SP_LBO, SP_SBO>(addr); }
 
 // Instruction descriptor: kind::f16, D = F32, A = B = BF16, both K-major,
 // N = 128, M = 128.
@@ -185,13 +121,6 @@ __device__ __forceinline__ void umma_bf16(uint32_t d_tmem, uint64_t a_desc, uint
       "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}"
       ::"r"(d_tmem), "l"(a_desc), "l"(b_desc), "r"(SP_IDESC), "r"(accumulate));
 }
-
-__device__ __forceinline__ void umma_commit(unsigned long long *bar) {
-  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
-               : "memory");
-}
-
-__device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
 
 // Byte offset of element (row r, k) in a K-major no-swizzle tile of SP_KC columns.
 __device__ __forceinline__ int tile_off(int r, int k) {
@@ -445,7 +374,7 @@ __device__ void mma_drain(SplitSmem &S, int *err) {
   umma_commit(&S.drain);
   const unsigned long long t0 = global_ns();
   while (!mbar_try_wait(&S.drain, 0)) {
-    if (global_ns() - t0 > SP_WAIT_NS) {
+    if (global_ns() - t0 > sm100::WAIT_NS) {
       atomicOr(err, 4);
       break;
     }
@@ -651,6 +580,18 @@ __global__ void p1_rowmax_kernel(const double *__restrict__ P1, int n_basis, int
 
 int rho1_split_smem_bytes() { return (int)sizeof(SplitSmem) + 1024; }
 
+// plan.d_rowmax[r + n_basis t] = max_c |P1(r, c, t)|: the per-row scales of
+// P1c used by both split paths.
+int p1_rowmax_launch(const Rho1Plan &plan, const double *P1, cudaStream_t stream) {
+  FRPA_CUDA_TRY(cudaMemsetAsync(plan.d_rowmax, 0, sizeof(double) * (size_t)plan.n_basis * plan.T, stream));
+  const int cols = 256;
+  dim3 rg((plan.n_basis + 255) / 256, (plan.n_basis + cols - 1) / cols, plan.T);
+  p1_rowmax_kernel<<<rg, 256, 0, stream>>>(P1, plan.n_basis, cols,
+                                           reinterpret_cast<unsigned long long *>(plan.d_rowmax));
+  FRPA_LAUNCH_CHECK();
+  return FRPA_OK;
+}
+
 int rho1_split_launch(const Rho1Plan &plan, int n_active, const double *wave, const double *gwave,
                       const double *P1, const double *bias, const double *gbias, double *rho, double *grad,
                       cudaStream_t stream) {
@@ -663,13 +604,7 @@ int rho1_split_launch(const Rho1Plan &plan, int n_active, const double *wave, co
   FRPA_CUDA_TRY(cudaMemsetAsync(
       grad, 0, sizeof(double) * 3 * (size_t)plan.n_max_batch_size * plan.n_batches * plan.T, stream));
   if (plan.n_items_split == 0) return FRPA_OK;
-  // per-row scales of P1
-  FRPA_CUDA_TRY(cudaMemsetAsync(plan.d_rowmax, 0, sizeof(double) * (size_t)plan.n_basis * plan.T, stream));
-  const int cols = 256;
-  dim3 rg((plan.n_basis + 255) / 256, (plan.n_basis + cols - 1) / cols, plan.T);
-  p1_rowmax_kernel<<<rg, 256, 0, stream>>>(P1, plan.n_basis, cols,
-                                           reinterpret_cast<unsigned long long *>(plan.d_rowmax));
-  FRPA_LAUNCH_CHECK();
+  FRPA_TRY(p1_rowmax_launch(plan, P1, stream));
   static int configured[64] = {0};
   const int smem = rho1_split_smem_bytes();
   if (plan.device >= 0 && plan.device < 64 && !configured[plan.device]) {

@@ -58,8 +58,12 @@ int frpa_version(void);
 int frpa_set_atom_tile_size(int T);
 int frpa_get_atom_tile_size(void);
 
-/* rho1 contraction mode used by the reference drop-ins. */
-enum { FRPA_RHO1_FP64 = 0, FRPA_RHO1_SPLIT_BF16 = 1 };
+/* rho1 contraction mode used by the reference drop-ins:
+ *   FRPA_RHO1_FP64        FP64 tensor-core tiles (DMMA), the reference's arithmetic;
+ *   FRPA_RHO1_SPLIT_BF16  five BF16 slices per operand on tcgen05 kind::f16, FP32 level sums;
+ *   FRPA_RHO1_SPLIT_I8    five signed 8-bit digits per operand on tcgen05 kind::i8, exact
+ *                         int32 level sums, operands packed by separate kernels. */
+enum { FRPA_RHO1_FP64 = 0, FRPA_RHO1_SPLIT_BF16 = 1, FRPA_RHO1_SPLIT_I8 = 2 };
 int frpa_set_rho1_mode(int mode);
 int frpa_get_rho1_mode(void);
 
@@ -246,14 +250,20 @@ int frpa_rho1_bias_part2(const frpa_rho1_plan *plan, int T, int n_atoms, int j_a
  *                               tile serves twice the points);
  *   FRPA_TUNE_FP64_CTAS_PER_SM  0 (as many as fit), 1, 2 or 3;
  *   FRPA_TUNE_SPLIT_TILE_POINTS 16..128 points per split-BF16 work item;
- *   FRPA_TUNE_ORDER             0 largest items first, 1 batch order.
+ *   FRPA_TUNE_ORDER             0 largest items first, 1 batch order;
+ *   FRPA_TUNE_SPLIT_I8_SCRATCH_MB  MiB of packed-operand scratch per group of
+ *                               batches in the split-int8 mode (default 4096;
+ *                               the batches are packed and contracted group by
+ *                               group, a batch larger than this is a group of
+ *                               its own).
  * Results are unchanged by every setting.  Setting rebuilds and re-uploads the
  * work lists (synchronous: call it outside any stream capture). */
 enum {
   FRPA_TUNE_FP64_TILE_POINTS = 1,
   FRPA_TUNE_FP64_CTAS_PER_SM = 2,
   FRPA_TUNE_SPLIT_TILE_POINTS = 3,
-  FRPA_TUNE_ORDER = 4
+  FRPA_TUNE_ORDER = 4,
+  FRPA_TUNE_SPLIT_I8_SCRATCH_MB = 5
 };
 int frpa_rho1_plan_set_tuning(frpa_rho1_plan *plan, int key, int value);
 int frpa_rho1_plan_get_tuning(const frpa_rho1_plan *plan, int key, int *value);
