@@ -111,7 +111,7 @@ struct I8Item {
   long long b_tstride;   // B bytes per perturbation
   int sa_off;            // first per-point scale of the item
   int sb_off;            // first per-row scale of the batch (t = 0)
-  int sb_tstride;        // per-row scales per perturbation (n_nt * 96)
+  int sb_tstride;        // per-row scales per perturbation (n_nt * 48)
   int pad_;
 };
 static_assert(sizeof(I8Item) == 80, "I8Item layout");
@@ -119,7 +119,7 @@ static_assert(sizeof(I8Item) == 80, "I8Item layout");
 // One N tile of one batch and perturbation, packed by one CTA.
 struct I8BTile {
   int ib_off, nc, jn, t;
-  int n_rows, n_kc, sb_off, pad_;  // rows of this tile (multiple of 16, <= 96)
+  int n_rows, n_kc, sb_off, pad_;  // rows of this tile (multiple of 16, <= 48)
   long long b_off;                 // bytes of the tile's first chunk
 };
 static_assert(sizeof(I8BTile) == 40, "I8BTile layout");
@@ -171,6 +171,7 @@ struct Rho1Plan {
   I8BTile *d_i8_tiles = nullptr;
   std::vector<I8Group> i8_groups;
   long long i8_budget = 4LL << 30;  // bytes of A + B scratch per group
+  int i8_wave4 = 0;                  // every batch's phi offset a multiple of 4 doubles
   unsigned char *d_i8_a = nullptr, *d_i8_b = nullptr;
   double *d_i8_sa = nullptr, *d_i8_sb = nullptr;
 };

@@ -23,17 +23,18 @@
 //   1. pack A: one CTA per work item (<= 128 points of one batch) finds the
 //      per-point scales and writes phi's five digit planes in the tcgen05
 //      shared-memory tile image (K-major, no swizzle, 8 x 16-byte core
-//      matrices), one 32-wide K chunk after another;
-//   2. pack B: one CTA per (batch, perturbation, N tile of <= 96 rows)
+//      matrices), one 32-wide K chunk after another, 16 points at a time;
+//   2. pack B: one CTA per (batch, perturbation, N tile of <= 48 rows)
 //      gathers P1c = P1[ib, ib] (lanes along P1's contiguous rows) and writes
 //      its digit planes the same way;
 //   3. contract: one persistent CTA per SM.  A loader thread moves each
-//      stage's A and B chunks into a 5-stage shared-memory ring with bulk
+//      stage's A and B chunks into a 4-stage shared-memory ring with bulk
 //      copies; an MMA thread issues the 15 tcgen05.mma.kind::i8 of a stage
-//      (M = 128 points, N <= 96 rows, K = 32) into the five accumulators
-//      (480 of 512 TMEM columns); 8 epilogue warps read them (tcgen05.ld),
-//      recombine in FP64 and contract with phi and grad phi (FP64, global
-//      memory, loads issued a chunk ahead).
+//      (M = 128 points, N <= 48 rows, K = 32) into the five accumulators of
+//      one of two sets (2 x 240 of 512 TMEM columns); 8 epilogue warps read a
+//      finished set (tcgen05.ld), recombine in FP64 and contract with phi and
+//      grad phi (FP64, 256-bit loads from global memory issued a chunk ahead)
+//      while the MMAs of the next tile fill the other set.
 // The packed operands cost a write and a read of ~5 bytes per P1c and phi
 // element, in exchange the contraction has no gathers, no conversions and
 // no register-staged loads on its critical path.  Every mbarrier wait is
@@ -51,23 +52,26 @@ namespace {
 using namespace sm100;
 
 constexpr int I8_M = 128;      // points per work item (TMEM lanes)
-constexpr int I8_N = 96;       // rows i per N tile (accumulator columns per level)
+constexpr int I8_N = 48;       // rows i per N tile (accumulator columns per level)
 constexpr int I8_KC = 32;      // K per stage: one kind::i8 instruction
 constexpr int I8_LEVELS = 5;   // digit levels s + u = 0..4
 constexpr int I8_SLICES = 5;   // digit planes per operand
-constexpr int I8_STAGES = 5;
+constexpr int I8_SETS = 2;     // accumulator sets: a tile's epilogue overlaps the next tile's MMAs
+constexpr int I8_STAGES = 4;
 constexpr int I8_EPI_WARPS = 8;  // warps 0..7: lane quarter w % 4, column half w / 4; warp 0 owns TMEM
+constexpr int I8_COLS = I8_N / 2;  // 24 accumulator columns per epilogue warp
 constexpr int I8_LOAD_WARP = 8;  // lane 0 issues the bulk copies
 constexpr int I8_MMA_WARP = 9;   // lane 0 issues the MMAs
 constexpr int I8_THREADS = 32 * 10;
 constexpr int I8_ROWB = I8_KC;                         // bytes per tile row of one plane
 constexpr int I8_A_PLANE = I8_M * I8_ROWB;             // 4096
-constexpr int I8_B_STAGE = I8_SLICES * I8_N * I8_ROWB;  // 15360
+constexpr int I8_B_STAGE = I8_SLICES * I8_N * I8_ROWB;  // 7680
 constexpr uint32_t I8_LBO = 128;                       // K-adjacent core matrices
 constexpr uint32_t I8_SBO = 256;                       // 8-row groups
 constexpr int I8_TMEM_COLS = 512;
+constexpr int I8_SET_COLS = I8_LEVELS * I8_N;          // 240
 
-static_assert(I8_LEVELS * I8_N <= I8_TMEM_COLS, "accumulators fit TMEM");
+static_assert(I8_SETS * I8_SET_COLS <= I8_TMEM_COLS, "accumulators fit TMEM");
 
 // Instruction descriptor: kind::i8, D = S32, A = B = signed 8-bit, both
 // K-major, M = 128; N is or-ed in per tile.
@@ -86,7 +90,7 @@ __device__ __forceinline__ void umma_i8(uint32_t d_tmem, uint64_t a_desc, uint64
       "l"(a_desc), "l"(b_desc), "r"(idesc), "r"(accumulate));
 }
 
-// Rows of N tile jn of a batch with nc compute functions: 96, the last one
+// Rows of N tile jn of a batch with nc compute functions: 48, the last one
 // the remainder rounded up to 16 (the MMA's N granularity).
 __host__ __device__ __forceinline__ int tile_rows(int nc, int jn, int n_nt) {
   return jn < n_nt - 1 ? I8_N : ((nc - I8_N * (n_nt - 1) + 15) / 16) * 16;
@@ -148,52 +152,61 @@ __device__ __forceinline__ void digits16(const double (&x)[16], double sc39, uin
 // ------------------------------------------------------------ pack kernels
 
 constexpr int PA_THREADS = 256;
+constexpr int PA_GROUP = 16;  // points per pass: their rows are re-read from L2, not DRAM
 
 // phi of one work item -> A scratch: chunk kc, plane s at
 // a_off + (5 kc + s) rows8 32 bytes; rows pn..rows8-1 and k >= nc are zero.
+// Sixteen points at a time: their scales (one warp per point, lanes along the
+// row), then their digits (one thread per row and 16-wide K group; a warp's
+// stores cover 512 contiguous bytes of a plane).
 __global__ void __launch_bounds__(PA_THREADS) i8_pack_a_kernel(const I8Item *__restrict__ items,
                                                                const double *__restrict__ wave,
                                                                unsigned char *__restrict__ a_scr,
                                                                double *__restrict__ sa) {
-  __shared__ double s_sc[I8_M];
+  __shared__ double s_sc[PA_GROUP];
   const I8Item W = items[blockIdx.x];
   const int nc = W.nc, pn = W.pn, rows8 = W.rows8, ncp = (nc + 3) & ~3;
   const double *phi = wave + W.wave_off + (long long)W.p0 * ncp;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  for (int p = warp; p < rows8; p += PA_THREADS / 32) {
-    double m = 0.0;
-    if (p < pn) {
-      const double *row = phi + (long long)p * ncp;
-      for (int k = lane; k < nc; k += 32) m = fmax(m, fabs(__ldg(row + k)));
-    }
-#pragma unroll
-    for (int o = 16; o; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
-    if (lane == 0) {
-      double sc39, s23;
-      digit_scale(m, &sc39, &s23);
-      s_sc[p] = sc39;
-      sa[W.sa_off + p] = s23;
-    }
-  }
-  __syncthreads();
-  const int units = W.n_kc * 2 * rows8;
   const long long chunk = (long long)I8_SLICES * rows8 * I8_ROWB;
-  for (int u = threadIdx.x; u < units; u += PA_THREADS) {
-    const int p = u % rows8, kg = (u / rows8) & 1, kc = u / (2 * rows8);
-    const int k0 = kc * I8_KC + kg * 16;
-    const double *row = phi + (long long)(p < pn ? p : 0) * ncp;
-    double x[16];
+  for (int g0 = 0; g0 < rows8; g0 += PA_GROUP) {
+    const int gn = min(PA_GROUP, rows8 - g0);  // 8 or 16
+    for (int r = warp; r < gn; r += PA_THREADS / 32) {
+      const int p = g0 + r;
+      double m = 0.0;
+      if (p < pn) {
+        const double *row = phi + (long long)p * ncp;
+        for (int k = lane; k < nc; k += 32) m = fmax(m, fabs(__ldg(row + k)));
+      }
 #pragma unroll
-    for (int j = 0; j < 16; ++j) x[j] = (p < pn && k0 + j < nc) ? __ldg(row + k0 + j) : 0.0;
-    uint4 plane[I8_SLICES];
-    digits16(x, s_sc[p], plane);
-    unsigned char *dst = a_scr + W.a_off + kc * chunk + plane_off(p, kg);
+      for (int o = 16; o; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+      if (lane == 0) {
+        double sc39, s23;
+        digit_scale(m, &sc39, &s23);
+        s_sc[r] = sc39;
+        sa[W.sa_off + p] = s23;
+      }
+    }
+    __syncthreads();
+    const int units = W.n_kc * 2 * gn;
+    for (int u = threadIdx.x; u < units; u += PA_THREADS) {
+      const int r = u % gn, kg = (u / gn) & 1, kc = u / (2 * gn), p = g0 + r;
+      const int k0 = kc * I8_KC + kg * 16;
+      const double *row = phi + (long long)(p < pn ? p : 0) * ncp;
+      double x[16];
 #pragma unroll
-    for (int s = 0; s < I8_SLICES; ++s) *reinterpret_cast<uint4 *>(dst + s * rows8 * I8_ROWB) = plane[s];
+      for (int j = 0; j < 16; ++j) x[j] = (p < pn && k0 + j < nc) ? __ldg(row + k0 + j) : 0.0;
+      uint4 plane[I8_SLICES];
+      digits16(x, s_sc[r], plane);
+      unsigned char *dst = a_scr + W.a_off + kc * chunk + plane_off(p, kg);
+#pragma unroll
+      for (int s = 0; s < I8_SLICES; ++s) *reinterpret_cast<uint4 *>(dst + s * rows8 * I8_ROWB) = plane[s];
+    }
+    __syncthreads();  // s_sc is rewritten by the next group
   }
 }
 
-constexpr int PB_THREADS = 2 * I8_N;  // 96 rows x two 16-wide halves of a K chunk
+constexpr int PB_THREADS = 2 * I8_N;  // 48 rows x two 16-wide halves of a K chunk
 
 // P1c rows of one N tile -> B scratch: chunk kc, plane s at
 // b_off + kc 5 n_rows 32 + s n_rows 32; rows >= nc and k >= nc are zero.
@@ -240,8 +253,8 @@ struct I8Smem {
   double partial[2][4][I8_M];              // upper column half's per-point sums
   unsigned long long full[I8_STAGES];
   unsigned long long empty[I8_STAGES];
-  unsigned long long acc_full;
-  unsigned long long acc_empty;
+  unsigned long long acc_full[I8_SETS];
+  unsigned long long acc_empty[I8_SETS];
   unsigned long long drain;
   unsigned long long ep_sum[2];   // partial sums published by the upper column half
   unsigned long long ep_free[2];  // partial-sum buffer released by the lower half
@@ -259,6 +272,7 @@ struct I8Params {
   const double *sa, *sb;
   double *rho, *grad;
   int *err;
+  int wave_vec;  // every phi / grad phi row starts on a 32-byte boundary: 256-bit loads
 };
 
 // Lane 0 of the loader warp: every stage's A planes (5 copies of rows8 x 32
@@ -274,12 +288,11 @@ __device__ void loader_role(const I8Params &P, I8Smem &S) {
         const int N = tile_rows(W.nc, jn, W.n_nt);
         const uint32_t b_bytes = (uint32_t)(I8_SLICES * N * I8_ROWB);
         const unsigned char *bsrc = P.b_scr + W.b_off + t * W.b_tstride + (long long)jn * W.n_kc * I8_B_STAGE;
-        const unsigned char *asrc = P.a_scr + W.a_off;
         for (int kc = 0; kc < W.n_kc; ++kc, ++fill) {
           const int st = fill % I8_STAGES;
           if (!mbar_wait(&S.empty[st], ((fill / I8_STAGES) & 1) ^ 1, abort_flag, P.err)) goto out;
           mbar_arrive_expect_tx(&S.full[st], I8_SLICES * a_bytes + b_bytes);
-          const unsigned char *a = asrc + (long long)kc * I8_SLICES * a_bytes;
+          const unsigned char *a = P.a_scr + W.a_off + (long long)kc * I8_SLICES * a_bytes;
 #pragma unroll
           for (int s = 0; s < I8_SLICES; ++s) bulk_g2s(S.A[st][s], a + s * a_bytes, a_bytes, &S.full[st]);
           bulk_g2s(S.B[st], bsrc + (long long)kc * b_bytes, b_bytes, &S.full[st]);
@@ -294,8 +307,7 @@ out:
 }
 
 // Lane 0 of the MMA warp: per N tile, all K chunks' 15 digit products into
-// the five level accumulators; with one accumulator set the MMAs of a tile
-// wait for the epilogue of the previous one.
+// the five level accumulators of the tile's set (sets alternate by tile).
 __device__ void mma_role(const I8Params &P, I8Smem &S, uint32_t tmem) {
   volatile int *abort_flag = &S.abort_flag;
   uint32_t fill = 0, tile_ctr = 0;
@@ -306,7 +318,9 @@ __device__ void mma_role(const I8Params &P, I8Smem &S, uint32_t tmem) {
       for (int jn = 0; jn < W.n_nt; ++jn, ++tile_ctr) {
         const int N = tile_rows(W.nc, jn, W.n_nt);
         const uint32_t idesc = idesc_n(N);
-        if (!mbar_wait(&S.acc_empty, (tile_ctr & 1) ^ 1, abort_flag, P.err)) goto out;
+        const int set = tile_ctr & 1;
+        const uint32_t dcol = tmem + (uint32_t)(set * I8_SET_COLS);
+        if (!mbar_wait(&S.acc_empty[set], ((tile_ctr >> 1) & 1) ^ 1, abort_flag, P.err)) goto out;
         tc_fence_after();
         for (int kc = 0; kc < W.n_kc; ++kc, ++fill) {
           const int st = fill % I8_STAGES;
@@ -325,13 +339,13 @@ __device__ void mma_role(const I8Params &P, I8Smem &S, uint32_t tmem) {
 #pragma unroll
             for (int u = 0; u < I8_SLICES; ++u)
               if (s + u < I8_LEVELS) {
-                umma_i8(tmem + (uint32_t)((s + u) * I8_N), a[s], b[u], idesc, first[s + u]);
+                umma_i8(dcol + (uint32_t)((s + u) * I8_N), a[s], b[u], idesc, first[s + u]);
                 first[s + u] = 1u;
               }
           umma_commit(&S.empty[st]);
           issued = true;
         }
-        umma_commit(&S.acc_full);
+        umma_commit(&S.acc_full[set]);
       }
   }
 out:
@@ -343,33 +357,60 @@ out:
 }
 
 // FP64 operands of one 8-column chunk of the epilogue: phi and grad phi at
-// rows i = i0..i0+7 of one point's column (zero past n_compute).
+// rows i0..i0+7 of one point's column.  Values at rows >= n_compute (the
+// row padding, possibly garbage) are masked where they are used.
 struct EpiRegs {
   double f[8], gx[8], gy[8], gz[8];
 };
 
+__device__ __forceinline__ void ld4(const double *p, double *v) {
+  asm volatile("ld.global.nc.L1::no_allocate.v4.f64 {%0,%1,%2,%3}, [%4];" : "=d"(v[0]), "=d"(v[1]), "=d"(v[2]), "=d"(v[3]) : "l"(p));
+}
+
 __device__ __forceinline__ void epi_load(EpiRegs &E, const double *__restrict__ phi, const double *__restrict__ gph,
-                                         int ncp, int nc, int i0, bool live) {
+                                         int ncp, int nc, int i0, bool live, bool vec) {
+  if (vec) {  // 32-byte loads: i0 and the row starts are multiples of 4, rows end at ncp >= i0 + 4
 #pragma unroll
-  for (int j = 0; j < 8; ++j) {
-    const bool ok = live && i0 + j < nc;
-    E.f[j] = ok ? __ldg(phi + i0 + j) : 0.0;
-    E.gx[j] = ok ? __ldg(gph + i0 + j) : 0.0;
-    E.gy[j] = ok ? __ldg(gph + i0 + j + ncp) : 0.0;
-    E.gz[j] = ok ? __ldg(gph + i0 + j + 2 * ncp) : 0.0;
+    for (int h = 0; h < 2; ++h) {
+      const int c = i0 + 4 * h;
+      if (live && c < nc) {
+        ld4(phi + c, &E.f[4 * h]);
+        ld4(gph + c, &E.gx[4 * h]);
+        ld4(gph + ncp + c, &E.gy[4 * h]);
+        ld4(gph + 2 * ncp + c, &E.gz[4 * h]);
+      } else {
+#pragma unroll
+        for (int e = 0; e < 4; ++e) E.f[4 * h + e] = E.gx[4 * h + e] = E.gy[4 * h + e] = E.gz[4 * h + e] = 0.0;
+      }
+    }
+  } else {
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+      const bool ok = live && i0 + j < nc;
+      E.f[j] = ok ? __ldg(phi + i0 + j) : 0.0;
+      E.gx[j] = ok ? __ldg(gph + i0 + j) : 0.0;
+      E.gy[j] = ok ? __ldg(gph + i0 + j + ncp) : 0.0;
+      E.gz[j] = ok ? __ldg(gph + i0 + j + 2 * ncp) : 0.0;
+    }
   }
 }
 
 // Epilogue warp w reads TMEM lanes 32 (w % 4).. (its points) and columns
-// 48 (w / 4)..+47 of each level accumulator; the two warps of a lane quarter
-// add their partial sums through shared memory at each perturbation's end.
+// 24 (w / 4)..+23 of each level accumulator of the tile's set, recombines the
+// five levels in FP64 and contracts with phi and grad phi; the loads of each
+// 8-column chunk are issued one chunk ahead (the first chunk of a tile
+// before its accumulators are waited for).  The set is released after the
+// last chunk; meanwhile the MMAs of the next tile fill the other set.  The
+// two warps of a lane quarter add their partial sums through shared memory
+// at each perturbation's end.
 __device__ void epilogue_role(const I8Params &P, I8Smem &S, uint32_t tmem, int warp, int lane) {
   int *err = P.err;
   volatile int *abort_flag = &S.abort_flag;
   const int quarter = warp & 3, half = warp >> 2;
-  const int p = quarter * 32 + lane;
+  const int p = quarter * 32 + lane;  // TMEM lane = point within the tile
   const uint32_t lane_base = tmem + ((uint32_t)(quarter * 32) << 16);
-  const int cbase = half * (I8_N / 2);
+  const int cbase = half * I8_COLS;
+  const bool vec = P.wave_vec != 0;
   uint32_t tile_ctr = 0, sum_ctr = 0;
   for (int it = blockIdx.x; it < P.n_items; it += gridDim.x) {
     const I8Item W = P.items[it];
@@ -378,40 +419,48 @@ __device__ void epilogue_role(const I8Params &P, I8Smem &S, uint32_t tmem, int w
     const long long pt = W.p0 + (live ? p : 0);
     const double *phi = P.wave + W.wave_off + pt * ncp;
     const double *gph = P.gwave + 3 * W.wave_off + 3 * pt * ncp;
-    const double sA = live ? P.sa[W.sa_off + p] : 0.0;
     for (int t = 0; t < P.T; ++t) {
       double r = 0.0, gx = 0.0, gy = 0.0, gz = 0.0;
       const double *sbt = P.sb + W.sb_off + (long long)t * W.sb_tstride;
       for (int jn = 0; jn < W.n_nt; ++jn, ++tile_ctr) {
         const int N = tile_rows(nc, jn, W.n_nt);
-        const int ncols = min(I8_N / 2, N - cbase);  // warp-uniform, a multiple of 8 (or <= 0)
+        const int ncols = min(I8_COLS, N - cbase);  // warp-uniform, a multiple of 8 (or <= 0)
         const int ibase = jn * I8_N + cbase;
+        const int set = tile_ctr & 1;
+        const uint32_t acc = lane_base + (uint32_t)(set * I8_SET_COLS + cbase);
         const double *sbv = sbt + ibase;
         EpiRegs E;
-        if (ncols > 0) epi_load(E, phi, gph, ncp, nc, ibase, live);  // before the wait
-        if (!warp_wait(&S.acc_full, tile_ctr & 1, abort_flag, err, lane)) return;
+        if (ncols > 0) epi_load(E, phi, gph, ncp, nc, ibase, live, vec);  // before the wait
+        if (!warp_wait(&S.acc_full[set], (tile_ctr >> 1) & 1, abort_flag, err, lane)) return;
         tc_fence_after();
 #pragma unroll 1
         for (int c = 0; c < ncols; c += 8) {
-          uint32_t v[I8_LEVELS][8];
+          const int lim = live ? nc - (ibase + c) : 0;  // rows of this chunk inside n_compute
 #pragma unroll
-          for (int q = 0; q < I8_LEVELS; ++q) tmem_ld8(lane_base + (uint32_t)(q * I8_N + cbase + c), v[q]);
-          tmem_wait_ld();
+          for (int hq = 0; hq < 8; hq += 4) {
+            uint32_t v[I8_LEVELS][4];
 #pragma unroll
-          for (int j = 0; j < 8; ++j) {
-            const long long h = (long long)(int)v[0][j] * 256 + (int)v[1][j];
-            const float lo = fmaf(fmaf((float)(int)v[2][j], 256.0f, (float)(int)v[3][j]), 256.0f, (float)(int)v[4][j]);
-            const double w = fma((double)h, 16777216.0, (double)lo) * __ldg(sbv + c + j);
-            r = fma(E.f[j], w, r);
-            gx = fma(E.gx[j], w, gx);
-            gy = fma(E.gy[j], w, gy);
-            gz = fma(E.gz[j], w, gz);
+            for (int l = 0; l < I8_LEVELS; ++l) tmem_ld4(acc + (uint32_t)(l * I8_N + c + hq), v[l]);
+            tmem_wait_ld();
+#pragma unroll
+            for (int e = 0; e < 4; ++e) {
+              const int j = hq + e;
+              const long long h = (long long)(int)v[0][e] * 256 + (int)v[1][e];
+              const float lo =
+                  fmaf(fmaf((float)(int)v[2][e], 256.0f, (float)(int)v[3][e]), 256.0f, (float)(int)v[4][e]);
+              const double w = fma((double)h, 16777216.0, (double)lo) * __ldg(sbv + c + j);
+              const bool ok = j < lim;
+              r = fma(ok ? E.f[j] : 0.0, w, r);
+              gx = fma(ok ? E.gx[j] : 0.0, w, gx);
+              gy = fma(ok ? E.gy[j] : 0.0, w, gy);
+              gz = fma(ok ? E.gz[j] : 0.0, w, gz);
+            }
           }
-          if (c + 8 < ncols) epi_load(E, phi, gph, ncp, nc, ibase + c + 8, live);
+          if (c + 8 < ncols) epi_load(E, phi, gph, ncp, nc, ibase + c + 8, live, vec);
         }
         tc_fence_before();
         __syncwarp();
-        if (lane == 0) mbar_arrive(&S.acc_empty);
+        if (lane == 0) mbar_arrive(&S.acc_empty[set]);
       }
       // combine the two column halves of this point and write
       const int sp = sum_ctr & 1;
@@ -430,6 +479,7 @@ __device__ void epilogue_role(const I8Params &P, I8Smem &S, uint32_t tmem, int w
         gz += S.partial[sp][3][p];
         mbar_arrive(&S.ep_free[sp]);
         if (live) {
+          const double sA = P.sa[W.sa_off + p];
           const int pp = W.p0 + p;
           const long long bidx = pp + (long long)P.n_max_batch_size * (W.batch + (long long)P.n_batches * t);
           P.grad[3 * bidx + 0] = (gx * sA) * 2 - P.gbias[3 * bidx + 0];
@@ -452,8 +502,10 @@ __global__ void __launch_bounds__(I8_THREADS, 1) rho1_i8_kernel(const I8Params P
       mbar_init(&S.full[s], 1);
       mbar_init(&S.empty[s], 1);
     }
-    mbar_init(&S.acc_full, 1);
-    mbar_init(&S.acc_empty, I8_EPI_WARPS);
+    for (int s = 0; s < I8_SETS; ++s) {
+      mbar_init(&S.acc_full[s], 1);
+      mbar_init(&S.acc_empty[s], I8_EPI_WARPS);
+    }
     mbar_init(&S.drain, 1);
     for (int h = 0; h < 2; ++h) {
       mbar_init(&S.ep_sum[h], I8_M);
@@ -561,6 +613,9 @@ int rho1_i8_build(Rho1Plan *plan) {
     g.tile1 = (int)tiles.size();
   }
   if (g.item1 > g.item0) groups.push_back(g);
+  plan->i8_wave4 = 1;
+  for (const Rho1WorkItem &bt : batches)
+    if (bt.wave_off & 3) plan->i8_wave4 = 0;
   cudaFree(plan->d_i8_items);
   cudaFree(plan->d_i8_tiles);
   plan->d_i8_items = nullptr;
@@ -654,6 +709,7 @@ int rho1_i8_launch(Rho1Plan &plan, int n_active, const double *wave, const doubl
   P.rho = rho;
   P.grad = grad;
   P.err = plan.d_err;
+  P.wave_vec = (plan.i8_wave4 && !(((uintptr_t)wave | (uintptr_t)gwave) & 31)) ? 1 : 0;
   for (const I8Group &g : plan.i8_groups) {
     const int ni = g.item1 - g.item0, nt = g.tile1 - g.tile0;
     i8_pack_a_kernel<<<ni, PA_THREADS, 0, stream>>>(plan.d_i8_items + g.item0, wave, plan.d_i8_a, plan.d_i8_sa);

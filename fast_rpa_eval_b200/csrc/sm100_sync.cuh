@@ -125,6 +125,13 @@ __device__ __forceinline__ void tmem_ld8(uint32_t taddr, uint32_t (&r)[8]) {
                : "r"(taddr));
 }
 
+// 4 consecutive 32-bit TMEM columns of this thread's lane.
+__device__ __forceinline__ void tmem_ld4(uint32_t taddr, uint32_t (&r)[4]) {
+  asm volatile("tcgen05.ld.sync.aligned.32x32b.x4.b32 {%0,%1,%2,%3}, [%4];"
+               : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3])
+               : "r"(taddr));
+}
+
 // Bulk copy global -> this CTA's shared memory, completing `bytes` on `bar`
 // (both addresses 16-byte aligned, bytes a multiple of 16).
 __device__ __forceinline__ void bulk_g2s(void *dst, const void *src, uint32_t bytes, unsigned long long *bar) {
@@ -132,6 +139,12 @@ __device__ __forceinline__ void bulk_g2s(void *dst, const void *src, uint32_t by
                    smem_u32(dst)),
                "l"(src), "r"(bytes), "r"(smem_u32(bar))
                : "memory");
+}
+
+// Asynchronous prefetch of [src, src + bytes) into L2 (src 16-byte aligned,
+// bytes a multiple of 16).
+__device__ __forceinline__ void l2_prefetch(const void *src, uint32_t bytes) {
+  asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(src), "r"(bytes) : "memory");
 }
 
 }  // namespace sm100
