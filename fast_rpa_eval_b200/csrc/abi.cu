@@ -156,6 +156,7 @@ static int rho1_plan_build(Rho1Plan **out, const frpa_rho1_desc *D) {
   };
   up((void **)&P->d_items, items.data(), sizeof(Rho1WorkItem) * items.size());
   P->h_batches = batches;
+  P->h_ib = ibc;
   {
     std::vector<Rho1WorkItem> split;
     rho1_split_build_items(batches, P->split_tile_points, P->order, &split);

@@ -165,6 +165,7 @@ struct Rho1Plan {
   int split_tile_points = 128; // <= 128 points per split-BF16 work item
   int order = 0;               // 0: largest items first, 1: batch order
   std::vector<Rho1WorkItem> h_batches;
+  std::vector<int> h_ib;  // host copy of the compact basis lists
   // split-int8 path: work lists (built with the plan) and the scratch
   // (allocated by the first split-int8 execution, reused afterwards)
   I8Item *d_i8_items = nullptr;

@@ -151,6 +151,13 @@ __device__ __forceinline__ void digits16(const double (&x)[16], double sc39, uin
 
 // ------------------------------------------------------------ pack kernels
 
+// Four doubles from a 32-byte aligned address, not kept in L1.
+__device__ __forceinline__ void ld4(const double *p, double *v) {
+  asm volatile("ld.global.nc.L1::no_allocate.v4.f64 {%0,%1,%2,%3}, [%4];"
+               : "=d"(v[0]), "=d"(v[1]), "=d"(v[2]), "=d"(v[3])
+               : "l"(p));
+}
+
 constexpr int PA_THREADS = 256;
 constexpr int PA_GROUP = 16;  // points per pass: their rows are re-read from L2, not DRAM
 
@@ -162,7 +169,7 @@ constexpr int PA_GROUP = 16;  // points per pass: their rows are re-read from L2
 __global__ void __launch_bounds__(PA_THREADS) i8_pack_a_kernel(const I8Item *__restrict__ items,
                                                                const double *__restrict__ wave,
                                                                unsigned char *__restrict__ a_scr,
-                                                               double *__restrict__ sa) {
+                                                               double *__restrict__ sa, int vec) {
   __shared__ double s_sc[PA_GROUP];
   const I8Item W = items[blockIdx.x];
   const int nc = W.nc, pn = W.pn, rows8 = W.rows8, ncp = (nc + 3) & ~3;
@@ -194,8 +201,22 @@ __global__ void __launch_bounds__(PA_THREADS) i8_pack_a_kernel(const I8Item *__r
       const int k0 = kc * I8_KC + kg * 16;
       const double *row = phi + (long long)(p < pn ? p : 0) * ncp;
       double x[16];
+      if (vec) {  // rows start on 32-byte boundaries; a vector that starts below nc ends by ncp
 #pragma unroll
-      for (int j = 0; j < 16; ++j) x[j] = (p < pn && k0 + j < nc) ? __ldg(row + k0 + j) : 0.0;
+        for (int v = 0; v < 4; ++v) {
+          if (p < pn && k0 + 4 * v < nc) {
+            ld4(row + k0 + 4 * v, &x[4 * v]);
+          } else {
+#pragma unroll
+            for (int e = 0; e < 4; ++e) x[4 * v + e] = 0.0;
+          }
+        }
+#pragma unroll
+        for (int j = 0; j < 16; ++j) x[j] = k0 + j < nc ? x[j] : 0.0;  // the row padding
+      } else {
+#pragma unroll
+        for (int j = 0; j < 16; ++j) x[j] = (p < pn && k0 + j < nc) ? __ldg(row + k0 + j) : 0.0;
+      }
       uint4 plane[I8_SLICES];
       digits16(x, s_sc[r], plane);
       unsigned char *dst = a_scr + W.a_off + kc * chunk + plane_off(p, kg);
@@ -362,10 +383,6 @@ out:
 struct EpiRegs {
   double f[8], gx[8], gy[8], gz[8];
 };
-
-__device__ __forceinline__ void ld4(const double *p, double *v) {
-  asm volatile("ld.global.nc.L1::no_allocate.v4.f64 {%0,%1,%2,%3}, [%4];" : "=d"(v[0]), "=d"(v[1]), "=d"(v[2]), "=d"(v[3]) : "l"(p));
-}
 
 __device__ __forceinline__ void epi_load(EpiRegs &E, const double *__restrict__ phi, const double *__restrict__ gph,
                                          int ncp, int nc, int i0, bool live, bool vec) {
@@ -553,9 +570,14 @@ int i8_smem_bytes() { return (int)sizeof(I8Smem) + 128; }
 // scratch stays within plan->i8_budget (a batch larger than that is a group
 // of its own).
 int rho1_i8_build(Rho1Plan *plan) {
+  // Groups follow the lexicographic order of the batches' (ascending) basis
+  // lists, so that batches over the same atoms are packed together and
+  // their P1c gathers meet in L2; inside a group the contraction takes the
+  // batches by decreasing cost (nc^2 np), a batch's point tiles adjacent.
   std::vector<Rho1WorkItem> batches = plan->h_batches;
-  std::stable_sort(batches.begin(), batches.end(), [](const Rho1WorkItem &a, const Rho1WorkItem &b) {
-    return (long long)a.nc * a.nc * a.np > (long long)b.nc * b.nc * b.np;
+  const int *ibh = plan->h_ib.data();
+  std::stable_sort(batches.begin(), batches.end(), [ibh](const Rho1WorkItem &a, const Rho1WorkItem &b) {
+    return std::lexicographical_compare(ibh + a.ib_off, ibh + a.ib_off + a.nc, ibh + b.ib_off, ibh + b.ib_off + b.nc);
   });
   const int T = plan->T;
   std::vector<I8Item> items;
@@ -613,6 +635,10 @@ int rho1_i8_build(Rho1Plan *plan) {
     g.tile1 = (int)tiles.size();
   }
   if (g.item1 > g.item0) groups.push_back(g);
+  for (const I8Group &q : groups)  // cost order inside each group (siblings stay adjacent)
+    std::stable_sort(items.begin() + q.item0, items.begin() + q.item1, [](const I8Item &a, const I8Item &b) {
+      return a.nc != b.nc ? a.nc > b.nc : a.batch < b.batch;
+    });
   plan->i8_wave4 = 1;
   for (const Rho1WorkItem &bt : batches)
     if (bt.wave_off & 3) plan->i8_wave4 = 0;
@@ -712,7 +738,8 @@ int rho1_i8_launch(Rho1Plan &plan, int n_active, const double *wave, const doubl
   P.wave_vec = (plan.i8_wave4 && !(((uintptr_t)wave | (uintptr_t)gwave) & 31)) ? 1 : 0;
   for (const I8Group &g : plan.i8_groups) {
     const int ni = g.item1 - g.item0, nt = g.tile1 - g.tile0;
-    i8_pack_a_kernel<<<ni, PA_THREADS, 0, stream>>>(plan.d_i8_items + g.item0, wave, plan.d_i8_a, plan.d_i8_sa);
+    i8_pack_a_kernel<<<ni, PA_THREADS, 0, stream>>>(plan.d_i8_items + g.item0, wave, plan.d_i8_a, plan.d_i8_sa,
+                                                    P.wave_vec);
     FRPA_LAUNCH_CHECK();
     i8_pack_b_kernel<<<nt, PB_THREADS, 0, stream>>>(plan.d_i8_tiles + g.tile0, plan.d_ib, P1, plan.d_rowmax,
                                                     plan.n_basis, plan.d_i8_b, plan.d_i8_sb);
