@@ -173,8 +173,12 @@ struct Rho1Plan {
   std::vector<I8Group> i8_groups;
   long long i8_budget = 4LL << 30;  // bytes of A + B scratch per group
   int i8_wave4 = 0;                  // every batch's phi offset a multiple of 4 doubles
-  unsigned char *d_i8_a = nullptr, *d_i8_b = nullptr;
-  double *d_i8_sa = nullptr, *d_i8_sb = nullptr;
+  // two scratch sets: group g is packed into set g % 2 on a side stream while
+  // group g - 1 is contracted on the caller's stream
+  unsigned char *d_i8_a[2] = {nullptr, nullptr}, *d_i8_b[2] = {nullptr, nullptr};
+  double *d_i8_sa[2] = {nullptr, nullptr}, *d_i8_sb[2] = {nullptr, nullptr};
+  cudaStream_t i8_side = nullptr;
+  cudaEvent_t i8_ev_start = nullptr, i8_ev_packed[2] = {nullptr, nullptr}, i8_ev_done[2] = {nullptr, nullptr};
 };
 
 // Work lists of a plan's valid batches (one entry per batch in `batches`).

@@ -656,23 +656,39 @@ int rho1_i8_build(Rho1Plan *plan) {
   return FRPA_OK;
 }
 
+static void i8_free_scratch(Rho1Plan *plan) {
+  for (int k = 0; k < 2; ++k) {
+    cudaFree(plan->d_i8_a[k]);
+    cudaFree(plan->d_i8_b[k]);
+    cudaFree(plan->d_i8_sa[k]);
+    cudaFree(plan->d_i8_sb[k]);
+    plan->d_i8_a[k] = plan->d_i8_b[k] = nullptr;
+    plan->d_i8_sa[k] = plan->d_i8_sb[k] = nullptr;
+  }
+}
+
 void rho1_i8_free(Rho1Plan *plan) {
   cudaFree(plan->d_i8_items);
   cudaFree(plan->d_i8_tiles);
-  cudaFree(plan->d_i8_a);
-  cudaFree(plan->d_i8_b);
-  cudaFree(plan->d_i8_sa);
-  cudaFree(plan->d_i8_sb);
   plan->d_i8_items = nullptr;
   plan->d_i8_tiles = nullptr;
-  plan->d_i8_a = plan->d_i8_b = nullptr;
-  plan->d_i8_sa = plan->d_i8_sb = nullptr;
+  i8_free_scratch(plan);
+  if (plan->i8_side) cudaStreamDestroy(plan->i8_side);
+  if (plan->i8_ev_start) cudaEventDestroy(plan->i8_ev_start);
+  for (int k = 0; k < 2; ++k) {
+    if (plan->i8_ev_packed[k]) cudaEventDestroy(plan->i8_ev_packed[k]);
+    if (plan->i8_ev_done[k]) cudaEventDestroy(plan->i8_ev_done[k]);
+    plan->i8_ev_packed[k] = plan->i8_ev_done[k] = nullptr;
+  }
+  plan->i8_side = nullptr;
+  plan->i8_ev_start = nullptr;
 }
 
-// The scratch of the largest group, allocated on first use (not while the
-// stream is being captured into a graph).
+// Scratch sets sized for the largest group (two when there are several
+// groups) and the side stream, created on first use (not while the stream is
+// being captured into a graph).
 static int i8_scratch(Rho1Plan &plan, cudaStream_t stream) {
-  if (plan.d_i8_a) return FRPA_OK;
+  if (plan.d_i8_a[0]) return FRPA_OK;
   cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
   FRPA_CUDA_TRY(cudaStreamIsCapturing(stream, &cap));
   if (cap != cudaStreamCaptureStatusNone)
@@ -687,16 +703,23 @@ static int i8_scratch(Rho1Plan &plan, cudaStream_t stream) {
     sa = std::max(sa, g.sa_len);
     sb = std::max(sb, g.sb_len);
   }
-  if (cudaMalloc((void **)&plan.d_i8_a, a) != cudaSuccess || cudaMalloc((void **)&plan.d_i8_b, b) != cudaSuccess ||
-      cudaMalloc((void **)&plan.d_i8_sa, sizeof(double) * sa) != cudaSuccess ||
-      cudaMalloc((void **)&plan.d_i8_sb, sizeof(double) * sb) != cudaSuccess) {
-    cudaFree(plan.d_i8_a);
-    cudaFree(plan.d_i8_b);
-    cudaFree(plan.d_i8_sa);
-    cudaFree(plan.d_i8_sb);
-    plan.d_i8_a = plan.d_i8_b = nullptr;
-    plan.d_i8_sa = plan.d_i8_sb = nullptr;
-    return fail(FRPA_ERR_OOM, "rho1 split-int8: scratch of %lld + %lld bytes could not be allocated", a, b);
+  const int sets = plan.i8_groups.size() > 1 ? 2 : 1;
+  for (int k = 0; k < sets; ++k)
+    if (cudaMalloc((void **)&plan.d_i8_a[k], a) != cudaSuccess ||
+        cudaMalloc((void **)&plan.d_i8_b[k], b) != cudaSuccess ||
+        cudaMalloc((void **)&plan.d_i8_sa[k], sizeof(double) * sa) != cudaSuccess ||
+        cudaMalloc((void **)&plan.d_i8_sb[k], sizeof(double) * sb) != cudaSuccess) {
+      i8_free_scratch(&plan);
+      return fail(FRPA_ERR_OOM, "rho1 split-int8: %d scratch sets of %lld + %lld bytes could not be allocated",
+                  sets, a, b);
+    }
+  if (!plan.i8_side) {
+    FRPA_CUDA_TRY(cudaStreamCreateWithFlags(&plan.i8_side, cudaStreamNonBlocking));
+    FRPA_CUDA_TRY(cudaEventCreateWithFlags(&plan.i8_ev_start, cudaEventDisableTiming));
+    for (int k = 0; k < 2; ++k) {
+      FRPA_CUDA_TRY(cudaEventCreateWithFlags(&plan.i8_ev_packed[k], cudaEventDisableTiming));
+      FRPA_CUDA_TRY(cudaEventCreateWithFlags(&plan.i8_ev_done[k], cudaEventDisableTiming));
+    }
   }
   return FRPA_OK;
 }
@@ -728,26 +751,38 @@ int rho1_i8_launch(Rho1Plan &plan, int n_active, const double *wave, const doubl
   P.gwave = gwave;
   P.bias = bias;
   P.gbias = gbias;
-  P.a_scr = plan.d_i8_a;
-  P.b_scr = plan.d_i8_b;
-  P.sa = plan.d_i8_sa;
-  P.sb = plan.d_i8_sb;
   P.rho = rho;
   P.grad = grad;
   P.err = plan.d_err;
   P.wave_vec = (plan.i8_wave4 && !(((uintptr_t)wave | (uintptr_t)gwave) & 31)) ? 1 : 0;
-  for (const I8Group &g : plan.i8_groups) {
-    const int ni = g.item1 - g.item0, nt = g.tile1 - g.tile0;
-    i8_pack_a_kernel<<<ni, PA_THREADS, 0, stream>>>(plan.d_i8_items + g.item0, wave, plan.d_i8_a, plan.d_i8_sa,
-                                                    P.wave_vec);
+  // group g: packed on the side stream into scratch set g % 2 (after the
+  // contraction of group g - 2 released it), contracted on the caller's
+  // stream; the side stream joins back before the last contraction
+  const int sets = plan.d_i8_a[1] ? 2 : 1;
+  FRPA_CUDA_TRY(cudaEventRecord(plan.i8_ev_start, stream));
+  FRPA_CUDA_TRY(cudaStreamWaitEvent(plan.i8_side, plan.i8_ev_start, 0));
+  const int n_groups = (int)plan.i8_groups.size();
+  for (int gi = 0; gi < n_groups; ++gi) {
+    const I8Group &g = plan.i8_groups[gi];
+    const int k = gi % sets, ni = g.item1 - g.item0, nt = g.tile1 - g.tile0;
+    if (gi >= sets) FRPA_CUDA_TRY(cudaStreamWaitEvent(plan.i8_side, plan.i8_ev_done[k], 0));
+    i8_pack_a_kernel<<<ni, PA_THREADS, 0, plan.i8_side>>>(plan.d_i8_items + g.item0, wave, plan.d_i8_a[k],
+                                                          plan.d_i8_sa[k], P.wave_vec);
     FRPA_LAUNCH_CHECK();
-    i8_pack_b_kernel<<<nt, PB_THREADS, 0, stream>>>(plan.d_i8_tiles + g.tile0, plan.d_ib, P1, plan.d_rowmax,
-                                                    plan.n_basis, plan.d_i8_b, plan.d_i8_sb);
+    i8_pack_b_kernel<<<nt, PB_THREADS, 0, plan.i8_side>>>(plan.d_i8_tiles + g.tile0, plan.d_ib, P1, plan.d_rowmax,
+                                                          plan.n_basis, plan.d_i8_b[k], plan.d_i8_sb[k]);
     FRPA_LAUNCH_CHECK();
+    FRPA_CUDA_TRY(cudaEventRecord(plan.i8_ev_packed[k], plan.i8_side));
+    FRPA_CUDA_TRY(cudaStreamWaitEvent(stream, plan.i8_ev_packed[k], 0));
     P.items = plan.d_i8_items + g.item0;
     P.n_items = ni;
+    P.a_scr = plan.d_i8_a[k];
+    P.b_scr = plan.d_i8_b[k];
+    P.sa = plan.d_i8_sa[k];
+    P.sb = plan.d_i8_sb[k];
     rho1_i8_kernel<<<std::min(n_sm, ni), I8_THREADS, smem, stream>>>(P);
     FRPA_LAUNCH_CHECK();
+    if (gi + sets < n_groups) FRPA_CUDA_TRY(cudaEventRecord(plan.i8_ev_done[k], stream));
   }
   return FRPA_OK;
 }

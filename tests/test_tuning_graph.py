@@ -93,12 +93,18 @@ def test_autotuner_picks_and_caches(tmp_path):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("mode", [_lib.RHO1_FP64, _lib.RHO1_SPLIT_BF16])
-def test_graph_replay_matches_direct_execution(mode):
+@pytest.mark.parametrize("mode,scratch_mb", [(_lib.RHO1_FP64, None), (_lib.RHO1_SPLIT_BF16, None),
+                                             (_lib.RHO1_SPLIT_I8, None), (_lib.RHO1_SPLIT_I8, 1)])
+def test_graph_replay_matches_direct_execution(mode, scratch_mb):
+    """For split-int8 also with a 1 MiB scratch budget: several groups, packed
+    on the plan's side stream (captured through event edges) into two
+    alternating scratch sets."""
     import torch
 
     p, a = _setup(seed=5)
     plan = _lib.Rho1Plan(p)
+    if scratch_mb is not None:
+        plan.set_tuning(split_i8_scratch_mb=scratch_mb)
     g = _lib.capture_graph(lambda: _run(plan, p, a, mode))
     g.replay()
     torch.cuda.synchronize()
