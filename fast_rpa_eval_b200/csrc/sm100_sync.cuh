@@ -141,11 +141,5 @@ __device__ __forceinline__ void bulk_g2s(void *dst, const void *src, uint32_t by
                : "memory");
 }
 
-// Asynchronous prefetch of [src, src + bytes) into L2 (src 16-byte aligned,
-// bytes a multiple of 16).
-__device__ __forceinline__ void l2_prefetch(const void *src, uint32_t bytes) {
-  asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(src), "r"(bytes) : "memory");
-}
-
 }  // namespace sm100
 }  // namespace frpa
