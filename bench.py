@@ -55,7 +55,7 @@ def parse_args():
     ap.add_argument("--config4-sizes", default="2000",
                     help="config-4 sweep sizes in atoms (comma list; 2000,10000,40000 for the full sweep)")
     ap.add_argument("--no-config4", action="store_true", help="skip the config-4 sweep")
-    ap.add_argument("--mode", choices=["fp64", "split"], default=None,
+    ap.add_argument("--mode", choices=["fp64", "split", "i8"], default=None,
                     help="headline rho1 path (default: split if built, else fp64)")
     return ap.parse_args()
 
@@ -438,7 +438,7 @@ def run_frpa(args, ranks: Ranks):
     stream = torch.cuda.current_stream()
     peaks = measured_peaks()
     mode_name = args.mode or "fp64"
-    mode = _lib.RHO1_SPLIT_BF16 if mode_name == "split" else _lib.RHO1_FP64
+    mode = {"split": _lib.RHO1_SPLIT_BF16, "i8": _lib.RHO1_SPLIT_I8}.get(mode_name, _lib.RHO1_FP64)
     out = {}
 
     w = Rho1Workload(args.batches, seed=2 + 7919 * ranks.rank)
@@ -459,9 +459,10 @@ def run_frpa(args, ranks: Ranks):
         out["autotune"] = {nm: {"choice": r["choice"], "timings_ms": r["timings"]} for nm, r in tuned.items()}
         tuned = {nm: r["choice"] for nm, r in tuned.items()}
     graphs = {m: _lib.capture_graph(lambda m=m: w.step(m, None))
-              for m in (_lib.RHO1_FP64, _lib.RHO1_SPLIT_BF16)}
+              for m in (_lib.RHO1_FP64, _lib.RHO1_SPLIT_BF16, _lib.RHO1_SPLIT_I8)}
 
     n_items_tuned = w.plan.info()["n_items"]
+    i8_groups = w.plan.i8_info()["groups"]
 
     # both rho1 paths are timed on the same inputs; the headline is --mode
     clocks = ClockSampler(ranks.local)
@@ -469,30 +470,44 @@ def run_frpa(args, ranks: Ranks):
     ms_fp64 = time_device_steps(lambda: graphs[_lib.RHO1_FP64].replay(), args.steps, args.warmup, ranks, stream)
     ms_split = time_device_steps(lambda: graphs[_lib.RHO1_SPLIT_BF16].replay(), args.steps, args.warmup, ranks,
                                  stream)
+    ms_i8 = time_device_steps(lambda: graphs[_lib.RHO1_SPLIT_I8].replay(), args.steps, args.warmup, ranks, stream)
     clk = clocks.stop()
     del graphs
-    ms = ms_fp64 if mode == _lib.RHO1_FP64 else ms_split
+    ms = {_lib.RHO1_FP64: ms_fp64, _lib.RHO1_SPLIT_BF16: ms_split, _lib.RHO1_SPLIT_I8: ms_i8}[mode]
 
     total_pts = ranks.sum(float(w.points))
     value = total_pts / (ms / 1e3)
     achieved_tf = w.flops / (ms_fp64 / 1e3) / 1e12
 
-    # split-BF16 against plain FP64 on the full workload, same inputs
-    w.step(_lib.RHO1_SPLIT_BF16, stream)
-    torch.cuda.synchronize()
-    rho_m, grad_m = w.rho.clone(), w.grad.clone()
+    # both split modes against plain FP64 on the full workload, same inputs
+    split_out = {}
+    for m in (_lib.RHO1_SPLIT_BF16, _lib.RHO1_SPLIT_I8):
+        w.step(m, stream)
+        torch.cuda.synchronize()
+        split_out[m] = (w.rho.clone(), w.grad.clone())
     w.step(_lib.RHO1_FP64, stream)
     torch.cuda.synchronize()
-    out["split_vs_fp64_normwise_rel"] = {
-        "rho1": float((rho_m - w.rho).abs().max() / w.rho.abs().max()),
-        "grad_rho1": float((grad_m - w.grad).abs().max() / w.grad.abs().max())}
+    for m, key in ((_lib.RHO1_SPLIT_BF16, "split_vs_fp64_normwise_rel"),
+                   (_lib.RHO1_SPLIT_I8, "split_i8_vs_fp64_normwise_rel")):
+        rho_m, grad_m = split_out[m]
+        out[key] = {"rho1": float((rho_m - w.rho).abs().max() / w.rho.abs().max()),
+                    "grad_rho1": float((grad_m - w.grad).abs().max() / w.grad.abs().max())}
     out["device_flags"] = w.plan.device_flags()
-    del rho_m, grad_m
+    del split_out
     out["rho1_split_bf16"] = {"pts_per_s": total_pts / (ms_split / 1e3), "ms_per_step": ms_split,
                               "speedup_vs_fp64": ms_fp64 / ms_split,
                               "hbm_gbs_algorithmic": w_bytes / (ms_split / 1e3) / 1e9,
                               "frac_of_measured_hbm": w_bytes / (ms_split / 1e3) / 1e9 / peaks["hbm_gbs"],
                               "bf16_equivalent_tflops": 15 * w_flops / (ms_split / 1e3) / 1e12}
+    i8_traffic = profile_traffic("rho1_split_i8_step")
+    out["rho1_split_i8"] = {
+        "pts_per_s": total_pts / (ms_i8 / 1e3), "ms_per_step": ms_i8, "speedup_vs_fp64": ms_fp64 / ms_i8,
+        "kernels_per_group": "pack A (phi digits), pack B (P1c digits), tcgen05.mma.kind::i8 contraction",
+        "groups": i8_groups,
+        "hbm_gbs_algorithmic": w_bytes / (ms_i8 / 1e3) / 1e9,
+        "dram_bytes_per_step": i8_traffic,
+        "dram_gbs_measured_traffic": i8_traffic / (ms_i8 / 1e3) / 1e9 if i8_traffic else None,
+        "frac_of_measured_hbm": (i8_traffic / (ms_i8 / 1e3) / 1e9 / peaks["hbm_gbs"]) if i8_traffic else None}
     out["rho1_fp64"] = {"pts_per_s": total_pts / (ms_fp64 / 1e3), "ms_per_step": ms_fp64,
                         "tflops_fp64": achieved_tf, "frac_of_measured_fp64_mma": achieved_tf / fp64_peak,
                         "hbm_gbs_algorithmic": w.bytes / (ms_fp64 / 1e3) / 1e9}
@@ -615,7 +630,8 @@ def run_frpa(args, ranks: Ranks):
                    "parallelism": f"weak, {args.gpus} independent shards"},
         "roofline": roofline,
         "clocks": clk,
-        "gpu_launches": args.steps * (1 if mode == _lib.RHO1_FP64 else 2),
+        "gpu_launches": args.steps * {_lib.RHO1_FP64: 1, _lib.RHO1_SPLIT_BF16: 2,
+                                      _lib.RHO1_SPLIT_I8: 1 + 3 * i8_groups}[mode],
         "cpu_baseline": cpu,
         "e2e": e2e,
         "measured_fp64_tflops": {"mma": fp64_peak, "fma": fma_peak},

@@ -206,6 +206,13 @@ class Rho1Plan:
         check(lib().frpa_rho1_plan_info(self.handle, out))
         return {"n_items": out[0], "n_valid_batches": out[1], "n_valid_points": out[2]}
 
+    def i8_info(self):
+        """Split-int8 grouping: groups (three launches each), work items,
+        packed P1c tiles, largest per-group A + B scratch in bytes."""
+        out = (c_ll * 4)()
+        check(lib().frpa_rho1_plan_i8_info(self.handle, out))
+        return {"groups": out[0], "items": out[1], "b_tiles": out[2], "scratch_bytes": out[3]}
+
     def execute(self, n_active, wave, gwave, P1, bias, gbias, rho, grad, mode=RHO1_FP64, stream=None):
         check(lib().frpa_rho1_execute(self.handle, c_int(mode), c_int(n_active), _ptr(wave), _ptr(gwave), _ptr(P1),
                                       _ptr(bias), _ptr(gbias), _ptr(rho), _ptr(grad), _stream(stream)))

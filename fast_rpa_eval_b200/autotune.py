@@ -36,6 +36,10 @@ SPLIT_SPACE = [
 
 
 def space(mode: int) -> list[dict]:
+    """Candidates per mode; the split-int8 mode has no shape tuning (its
+    scratch budget changes how batches are grouped, not the speed)."""
+    if mode == _lib.RHO1_SPLIT_I8:
+        return [{}]
     return FP64_SPACE if mode == _lib.RHO1_FP64 else SPLIT_SPACE
 
 

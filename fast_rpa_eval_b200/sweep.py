@@ -62,9 +62,9 @@ def run_sweep(n_atoms: int, seed: int = 4, reps: int = 3, max_batches: int = 500
     geom = synth.config4_geometry(n_atoms, seed=seed)
     chunks = synth.sweep_chunks(geom, max_batches=max_batches, max_window=max_window)
     t_geom = time.time() - t0
-    ms = {_lib.RHO1_FP64: 0.0, _lib.RHO1_SPLIT_BF16: 0.0}
+    ms = {_lib.RHO1_FP64: 0.0, _lib.RHO1_SPLIT_BF16: 0.0, _lib.RHO1_SPLIT_I8: 0.0}
     pts = 0
-    err = {"rho1": 0.0, "grad_rho1": 0.0}
+    err = {m: {"rho1": 0.0, "grad_rho1": 0.0} for m in (_lib.RHO1_SPLIT_BF16, _lib.RHO1_SPLIT_I8)}
     choice = {}
     windows = []
     flags = 0
@@ -72,7 +72,7 @@ def run_sweep(n_atoms: int, seed: int = 4, reps: int = 3, max_batches: int = 500
         c = ChunkRun(geom, b0, b1, p1_seed)
         windows.append(c.prob.n_basis)
         if tune and ci == 0:
-            for m in ms:
+            for m in (_lib.RHO1_FP64, _lib.RHO1_SPLIT_BF16):
                 choice.update(autotune.tune_rho1(c.plan, c.prob, lambda m=m: c.step(m), m, reps=1)["choice"])
         elif choice:
             c.plan.set_tuning(**choice)
@@ -90,9 +90,11 @@ def run_sweep(n_atoms: int, seed: int = 4, reps: int = 3, max_batches: int = 500
             torch.cuda.synchronize()
             ms[m] += e0.elapsed_time(e1) / reps
             del g
-        (rf, gf), (rs, gs) = out[_lib.RHO1_FP64], out[_lib.RHO1_SPLIT_BF16]
-        err["rho1"] = max(err["rho1"], float((rs - rf).abs().max() / rf.abs().max()))
-        err["grad_rho1"] = max(err["grad_rho1"], float((gs - gf).abs().max() / gf.abs().max()))
+        rf, gf = out[_lib.RHO1_FP64]
+        for m, e in err.items():
+            rs, gs = out[m]
+            e["rho1"] = max(e["rho1"], float((rs - rf).abs().max() / rf.abs().max()))
+            e["grad_rho1"] = max(e["grad_rho1"], float((gs - gf).abs().max() / gf.abs().max()))
         flags |= c.plan.device_flags()
         pts += c.prob.total_points()
         del c, out
@@ -102,5 +104,7 @@ def run_sweep(n_atoms: int, seed: int = 4, reps: int = 3, max_batches: int = 500
         "max_window_functions": int(max(windows)), "tuning": choice or "defaults",
         "fp64": {"ms": ms[_lib.RHO1_FP64], "pts_per_s": pts / (ms[_lib.RHO1_FP64] / 1e3)},
         "split_bf16": {"ms": ms[_lib.RHO1_SPLIT_BF16], "pts_per_s": pts / (ms[_lib.RHO1_SPLIT_BF16] / 1e3)},
-        "split_vs_fp64_normwise_rel_max_over_chunks": err, "device_flags": flags,
+        "split_i8": {"ms": ms[_lib.RHO1_SPLIT_I8], "pts_per_s": pts / (ms[_lib.RHO1_SPLIT_I8] / 1e3)},
+        "split_vs_fp64_normwise_rel_max_over_chunks": err[_lib.RHO1_SPLIT_BF16],
+        "split_i8_vs_fp64_normwise_rel_max_over_chunks": err[_lib.RHO1_SPLIT_I8], "device_flags": flags,
         "host_geometry_s": t_geom}

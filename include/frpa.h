@@ -222,6 +222,10 @@ int frpa_rho1_plan_create(frpa_rho1_plan **plan, const frpa_rho1_desc *desc);
 int frpa_rho1_plan_destroy(frpa_rho1_plan *plan);
 /* Work-list statistics: [n_items, n_valid_batches, n_valid_points]. */
 int frpa_rho1_plan_info(const frpa_rho1_plan *plan, long long *info3);
+/* Split-int8 mode: [groups, work items, packed P1c tiles, largest A + B scratch
+ * of a group in bytes] (no counterpart in the reference).  Each group is three
+ * kernel launches (pack phi, pack P1c, contraction). */
+int frpa_rho1_plan_i8_info(const frpa_rho1_plan *plan, long long *info4);
 
 /* rho1 and grad rho1 for perturbations t < T; rho1 is written for
  * t < n_active = j_atom_end - j_atom_begin + 1 (evaluate_first_order_rho.cpp:202-207).

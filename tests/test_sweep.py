@@ -36,7 +36,8 @@ def test_chunk_problem_maps_back_to_the_global_functions():
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("mode,tol", [(_lib.RHO1_FP64, 1e-12), (_lib.RHO1_SPLIT_BF16, 1e-10)])
+@pytest.mark.parametrize("mode,tol", [(_lib.RHO1_FP64, 1e-12), (_lib.RHO1_SPLIT_BF16, 1e-10),
+                                      (_lib.RHO1_SPLIT_I8, 1e-10)])
 def test_chunk_matches_oracle(mode, tol):
     import torch
 
@@ -81,3 +82,4 @@ def test_small_sweep_end_to_end():
     res = sweep.run_sweep(30, reps=1, max_batches=80, max_window=500)
     assert res["chunks"] >= 2 and res["grid_points"] > 0 and res["device_flags"] == 0
     assert res["split_vs_fp64_normwise_rel_max_over_chunks"]["rho1"] < 1e-10
+    assert res["split_i8_vs_fp64_normwise_rel_max_over_chunks"]["rho1"] < 1e-10
