@@ -535,6 +535,12 @@ def run_frpa(args, ranks: Ranks):
                "d2h_bytes_per_step": d2h, "ms_per_step": ms_e2e,
                "call": "evaluate_first_order_rho_reduce_memory_c_v3_batches_atoms_cu_host_ (pinned host P1, biases, "
                        "outputs; phi resident)", "outputs_finite": finite}
+        if mode != _lib.RHO1_SPLIT_I8:  # the same call with the drop-ins switched to split-int8
+            ms8, h2d8, d2h8, finite8 = time_e2e(w, _lib.RHO1_SPLIT_I8, max(3, args.steps // 2), args.warmup, ranks)
+            out["e2e_split_i8"] = {"value": total_pts / (ms8 / 1e3), "unit": UNIT, "h2d_bytes_per_step": h2d8,
+                                   "d2h_bytes_per_step": d2h8, "ms_per_step": ms8,
+                                   "call": "same entry point after frpa_set_rho1_mode(FRPA_RHO1_SPLIT_I8)",
+                                   "outputs_finite": finite8}
 
     # CPU baseline on rank 0 at N = 1: the reference's CPU code, same batches
     cpu = None

@@ -111,7 +111,7 @@ struct I8Item {
   long long b_tstride;   // B bytes per perturbation
   int sa_off;            // first per-point scale of the item
   int sb_off;            // first per-row scale of the batch (t = 0)
-  int sb_tstride;        // per-row scales per perturbation (n_nt * 48)
+  int sb_tstride;        // per-row scales per perturbation (n_nt * 32)
   int pad_;
 };
 static_assert(sizeof(I8Item) == 80, "I8Item layout");
@@ -119,7 +119,7 @@ static_assert(sizeof(I8Item) == 80, "I8Item layout");
 // One N tile of one batch and perturbation, packed by one CTA.
 struct I8BTile {
   int ib_off, nc, jn, t;
-  int n_rows, n_kc, sb_off, pad_;  // rows of this tile (multiple of 16, <= 48)
+  int n_rows, n_kc, sb_off, pad_;  // rows of this tile (multiple of 16, <= 32)
   long long b_off;                 // bytes of the tile's first chunk
 };
 static_assert(sizeof(I8BTile) == 40, "I8BTile layout");

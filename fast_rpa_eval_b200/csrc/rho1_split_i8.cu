@@ -11,27 +11,28 @@
 // and written in balanced base 256, X = a0 2^32 + a1 2^24 + a2 2^16 +
 // a3 2^8 + a4, every digit a signed byte (|a0| <= 127 since
 // |X| < 2^39 - 2^31 - 2^23 - 2^15 - 2^7).  The product of two rows is the sum
-// of the 15 digit products with s + u <= 4, accumulated per level L = s + u
-// in five int32 TMEM accumulators; |a_s b_u| <= 2^14, so every level stays
-// exact for K < 26,000.  Recombined in FP64:
-//   work1(i, p) = 2^(eA + eB - 46) (L0 2^32 + L1 2^24 + L2 2^16 + L3 2^8 + L4).
+// of the 19 digit products with s + u <= 5, accumulated per level L = s + u
+// in six int32 TMEM accumulators; |a_s b_u| <= 2^14, so every level stays
+// exact for K < 26,000 (at most five products per level).  Recombined in FP64:
+//   work1(i, p) = 2^(eA + eB - 54) (L0 2^40 + L1 2^32 + L2 2^24 + L3 2^16 + L4 2^8 + L5).
 // What remains is the rounding of the operands to 2^-40 of their row scale
-// and the dropped levels 5..8 (below 2^-40 per product): ~1e-11 normwise on
-// the benchmark recipes.
+// and the dropped levels 6..8 (2^-48 per product); keeping level 5 removes
+// the error term that dominated with levels 0..4 only (3.5x larger than the
+// operand rounding in a CPU emulation of these steps).
 //
 // Data flow, three launches per group of batches:
 //   1. pack A: one CTA per work item (<= 128 points of one batch) finds the
 //      per-point scales and writes phi's five digit planes in the tcgen05
 //      shared-memory tile image (K-major, no swizzle, 8 x 16-byte core
 //      matrices), one 32-wide K chunk after another, 16 points at a time;
-//   2. pack B: one CTA per (batch, perturbation, N tile of <= 48 rows)
+//   2. pack B: one CTA per (batch, perturbation, N tile of <= 32 rows)
 //      gathers P1c = P1[ib, ib] (lanes along P1's contiguous rows) and writes
 //      its digit planes the same way;
 //   3. contract: one persistent CTA per SM.  A loader thread moves each
 //      stage's A and B chunks into a 4-stage shared-memory ring with bulk
-//      copies; an MMA thread issues the 15 tcgen05.mma.kind::i8 of a stage
-//      (M = 128 points, N <= 48 rows, K = 32) into the five accumulators of
-//      one of two sets (2 x 240 of 512 TMEM columns); 8 epilogue warps read a
+//      copies; an MMA thread issues the 19 tcgen05.mma.kind::i8 of a stage
+//      (M = 128 points, N <= 32 rows, K = 32) into the six accumulators of
+//      one of two sets (2 x 192 of 512 TMEM columns); 8 epilogue warps read a
 //      finished set (tcgen05.ld), recombine in FP64 and contract with phi and
 //      grad phi (FP64, 256-bit loads from global memory issued a chunk ahead)
 //      while the MMAs of the next tile fill the other set.
@@ -52,24 +53,24 @@ namespace {
 using namespace sm100;
 
 constexpr int I8_M = 128;      // points per work item (TMEM lanes)
-constexpr int I8_N = 48;       // rows i per N tile (accumulator columns per level)
+constexpr int I8_N = 32;       // rows i per N tile (accumulator columns per level)
 constexpr int I8_KC = 32;      // K per stage: one kind::i8 instruction
-constexpr int I8_LEVELS = 5;   // digit levels s + u = 0..4
+constexpr int I8_LEVELS = 6;   // digit levels s + u = 0..5
 constexpr int I8_SLICES = 5;   // digit planes per operand
 constexpr int I8_SETS = 2;     // accumulator sets: a tile's epilogue overlaps the next tile's MMAs
 constexpr int I8_STAGES = 4;
 constexpr int I8_EPI_WARPS = 8;  // warps 0..7: lane quarter w % 4, column half w / 4; warp 0 owns TMEM
-constexpr int I8_COLS = I8_N / 2;  // 24 accumulator columns per epilogue warp
+constexpr int I8_COLS = I8_N / 2;  // 16 accumulator columns per epilogue warp
 constexpr int I8_LOAD_WARP = 8;  // lane 0 issues the bulk copies
 constexpr int I8_MMA_WARP = 9;   // lane 0 issues the MMAs
 constexpr int I8_THREADS = 32 * 10;
 constexpr int I8_ROWB = I8_KC;                         // bytes per tile row of one plane
 constexpr int I8_A_PLANE = I8_M * I8_ROWB;             // 4096
-constexpr int I8_B_STAGE = I8_SLICES * I8_N * I8_ROWB;  // 7680
+constexpr int I8_B_STAGE = I8_SLICES * I8_N * I8_ROWB;  // 5120
 constexpr uint32_t I8_LBO = 128;                       // K-adjacent core matrices
 constexpr uint32_t I8_SBO = 256;                       // 8-row groups
 constexpr int I8_TMEM_COLS = 512;
-constexpr int I8_SET_COLS = I8_LEVELS * I8_N;          // 240
+constexpr int I8_SET_COLS = I8_LEVELS * I8_N;          // 192
 
 static_assert(I8_SETS * I8_SET_COLS <= I8_TMEM_COLS, "accumulators fit TMEM");
 
@@ -90,7 +91,7 @@ __device__ __forceinline__ void umma_i8(uint32_t d_tmem, uint64_t a_desc, uint64
       "l"(a_desc), "l"(b_desc), "r"(idesc), "r"(accumulate));
 }
 
-// Rows of N tile jn of a batch with nc compute functions: 48, the last one
+// Rows of N tile jn of a batch with nc compute functions: 32, the last one
 // the remainder rounded up to 16 (the MMA's N granularity).
 __host__ __device__ __forceinline__ int tile_rows(int nc, int jn, int n_nt) {
   return jn < n_nt - 1 ? I8_N : ((nc - I8_N * (n_nt - 1) + 15) / 16) * 16;
@@ -227,7 +228,7 @@ __global__ void __launch_bounds__(PA_THREADS) i8_pack_a_kernel(const I8Item *__r
   }
 }
 
-constexpr int PB_THREADS = 2 * I8_N;  // 48 rows x two 16-wide halves of a K chunk
+constexpr int PB_THREADS = 2 * I8_N;  // 32 rows x two 16-wide halves of a K chunk
 
 // P1c rows of one N tile -> B scratch: chunk kc, plane s at
 // b_off + kc 5 n_rows 32 + s n_rows 32; rows >= nc and k >= nc are zero.
@@ -250,7 +251,7 @@ __global__ void __launch_bounds__(PB_THREADS) i8_pack_b_kernel(const I8BTile *__
   const double *P1t = P1 + (long long)n_basis * n_basis * B.t;
   double sc39, s23;
   digit_scale(rok ? __ldg(rowmax + ibr + (long long)n_basis * B.t) : 0.0, &sc39, &s23);
-  if (kg == 0) sb[B.sb_off + r] = rok ? s23 : 0.0;
+  if (kg == 0) sb[B.sb_off + r] = rok ? s23 * 0.00390625 : 0.0;  // 2^(e - 31): the recombination sums 256 S
   const long long chunk = (long long)I8_SLICES * N * I8_ROWB;
   for (int kc = 0; kc < B.n_kc; ++kc) {
     const int k0 = kc * I8_KC + kg * 16;
@@ -328,7 +329,7 @@ out:
 }
 
 // Lane 0 of the MMA warp: per N tile, all K chunks' 15 digit products into
-// the five level accumulators of the tile's set (sets alternate by tile).
+// the six level accumulators of the tile's set (sets alternate by tile).
 __device__ void mma_role(const I8Params &P, I8Smem &S, uint32_t tmem) {
   volatile int *abort_flag = &S.abort_flag;
   uint32_t fill = 0, tile_ctr = 0;
@@ -353,8 +354,9 @@ __device__ void mma_role(const I8Params &P, I8Smem &S, uint32_t tmem) {
             a[s] = smem_desc<I8_LBO, I8_SBO>(smem_u32(S.A[st][s]));
             b[s] = smem_desc<I8_LBO, I8_SBO>(smem_u32(S.B[st]) + (uint32_t)(s * N * I8_ROWB));
           }
-          const uint32_t acc = kc > 0 ? 1u : 0u;
-          uint32_t first[I8_LEVELS] = {acc, acc, acc, acc, acc};
+          uint32_t first[I8_LEVELS];
+#pragma unroll
+          for (int l = 0; l < I8_LEVELS; ++l) first[l] = kc > 0 ? 1u : 0u;
 #pragma unroll
           for (int s = 0; s < I8_SLICES; ++s)
 #pragma unroll
@@ -413,8 +415,8 @@ __device__ __forceinline__ void epi_load(EpiRegs &E, const double *__restrict__ 
 }
 
 // Epilogue warp w reads TMEM lanes 32 (w % 4).. (its points) and columns
-// 24 (w / 4)..+23 of each level accumulator of the tile's set, recombines the
-// five levels in FP64 and contracts with phi and grad phi; the loads of each
+// 16 (w / 4)..+15 of each level accumulator of the tile's set, recombines the
+// six levels in FP64 and contracts with phi and grad phi; the loads of each
 // 8-column chunk are issued one chunk ahead (the first chunk of a tile
 // before its accumulators are waited for).  The set is released after the
 // last chunk; meanwhile the MMAs of the next tile fill the other set.  The
@@ -462,10 +464,12 @@ __device__ void epilogue_role(const I8Params &P, I8Smem &S, uint32_t tmem, int w
 #pragma unroll
             for (int e = 0; e < 4; ++e) {
               const int j = hq + e;
-              const long long h = (long long)(int)v[0][e] * 256 + (int)v[1][e];
-              const float lo =
-                  fmaf(fmaf((float)(int)v[2][e], 256.0f, (float)(int)v[3][e]), 256.0f, (float)(int)v[4][e]);
-              const double w = fma((double)h, 16777216.0, (double)lo) * __ldg(sbv + c + j);
+              // 256 S = (L0 256 + L1) 2^32 + (L2 256 + L3) 2^16 + (L4 256 + L5), each pair exact in int64
+              const long long hi = (long long)(int)v[0][e] * 256 + (int)v[1][e];
+              const long long mid = (long long)(int)v[2][e] * 256 + (int)v[3][e];
+              const long long lo = (long long)(int)v[4][e] * 256 + (int)v[5][e];
+              const double w = fma((double)hi, 4294967296.0, fma((double)mid, 65536.0, (double)lo)) *
+                               __ldg(sbv + c + j);
               const bool ok = j < lim;
               r = fma(ok ? E.f[j] : 0.0, w, r);
               gx = fma(ok ? E.gx[j] : 0.0, w, gx);

@@ -85,3 +85,32 @@ def test_i8_deterministic_and_scaled_inputs():
     r, g = run_i8(p)
     r_o, g_o = oracle.rho1(p)
     assert normwise_rel(r, r_o) < TOL_SPLIT and normwise_rel(g, g_o) < TOL_SPLIT
+
+
+@pytest.mark.parametrize("via", ["dropin", "session"])
+def test_i8_through_the_reference_entry_points(via):
+    """frpa_set_rho1_mode(FRPA_RHO1_SPLIT_I8) switches the reference-named
+    entry points (the host drop-in and the session's cu_host twin) to this
+    mode; two calls in a row, P1 changed in between."""
+    p = synth.make_rho1_problem(T=2, seed=43, with_bias=True, extra_full_points=5, empty_batches=2)
+    _lib.set_rho1_mode(_lib.RHO1_SPLIT_I8)
+    try:
+        if via == "dropin":
+            outs = []
+            for rep in range(2):
+                q = synth.make_rho1_problem(T=2, seed=43, with_bias=True, extra_full_points=5, empty_batches=2)
+                q.first_order_density_matrix = np.asfortranarray(q.first_order_density_matrix * (1.0 + rep))
+                outs.append((q, _lib.dropin_rho1(q)))
+        else:
+            outs = []
+            with _lib.Session(p) as s:
+                for rep in range(2):
+                    q = synth.make_rho1_problem(T=2, seed=43, with_bias=True, extra_full_points=5, empty_batches=2)
+                    q.first_order_density_matrix = np.asfortranarray(p.first_order_density_matrix * (1.0 + rep))
+                    outs.append((q, s.rho1(P1=q.first_order_density_matrix)))
+    finally:
+        _lib.set_rho1_mode(_lib.RHO1_FP64)
+    for q, (r, g) in outs:
+        r_o, g_o = oracle.rho1(q)
+        assert normwise_rel(r.reshape(r_o.shape, order="F"), r_o) < TOL_SPLIT
+        assert normwise_rel(g.reshape(g_o.shape, order="F"), g_o) < TOL_SPLIT
