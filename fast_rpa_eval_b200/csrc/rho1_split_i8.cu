@@ -30,9 +30,11 @@
 //      its digit planes the same way;
 //   3. contract: one persistent CTA per SM.  A loader thread moves each
 //      stage's A and B chunks into a 4-stage shared-memory ring with bulk
-//      copies; an MMA thread issues the 19 tcgen05.mma.kind::i8 of a stage
-//      (M = 128 points, N <= 32 rows, K = 32) into the six accumulators of
-//      one of two sets (2 x 192 of 512 TMEM columns); 8 epilogue warps read a
+//      copies; an MMA thread issues a stage's 19 digit products as five
+//      tcgen05.mma.kind::i8 (M = 128 points, K = 32; the digit levels run
+//      along N: A plane s times B planes 0..5-s, N = 32 (6 - s) rows, into
+//      the six level accumulators from level s on) in one of two sets
+//      (2 x 192 of 512 TMEM columns); 8 epilogue warps read a
 //      finished set (tcgen05.ld), recombine in FP64 and contract with phi and
 //      grad phi (FP64, 256-bit loads from global memory issued a chunk ahead)
 //      while the MMAs of the next tile fill the other set.
@@ -66,7 +68,8 @@ constexpr int I8_MMA_WARP = 9;   // lane 0 issues the MMAs
 constexpr int I8_THREADS = 32 * 10;
 constexpr int I8_ROWB = I8_KC;                         // bytes per tile row of one plane
 constexpr int I8_A_PLANE = I8_M * I8_ROWB;             // 4096
-constexpr int I8_B_STAGE = I8_SLICES * I8_N * I8_ROWB;  // 5120
+constexpr int I8_B_STAGE = I8_SLICES * I8_N * I8_ROWB;  // 5120: the five planes of a stage's B chunk
+constexpr int I8_B_SLOT = I8_B_STAGE + I8_N * I8_ROWB;  // 6144: plus a zero plane (see mma_role)
 constexpr uint32_t I8_LBO = 128;                       // K-adjacent core matrices
 constexpr uint32_t I8_SBO = 256;                       // 8-row groups
 constexpr int I8_TMEM_COLS = 512;
@@ -91,11 +94,9 @@ __device__ __forceinline__ void umma_i8(uint32_t d_tmem, uint64_t a_desc, uint64
       "l"(a_desc), "l"(b_desc), "r"(idesc), "r"(accumulate));
 }
 
-// Rows of N tile jn of a batch with nc compute functions: 32, the last one
-// the remainder rounded up to 16 (the MMA's N granularity).
-__host__ __device__ __forceinline__ int tile_rows(int nc, int jn, int n_nt) {
-  return jn < n_nt - 1 ? I8_N : ((nc - I8_N * (n_nt - 1) + 15) / 16) * 16;
-}
+// Every N tile has 32 rows; the last one of a batch is padded with zero rows
+// (the B planes of all tiles then share one layout: plane u at rows 32 u).
+__host__ __device__ __forceinline__ int tile_rows(int, int, int) { return I8_N; }
 
 // Byte offset of (row r, K half kg) inside one plane of a tile.
 __device__ __forceinline__ int plane_off(int r, int kg) { return (r >> 3) * (int)I8_SBO + kg * 128 + (r & 7) * 16; }
@@ -271,7 +272,7 @@ __global__ void __launch_bounds__(PB_THREADS) i8_pack_b_kernel(const I8BTile *__
 
 struct I8Smem {
   unsigned char A[I8_STAGES][I8_SLICES][I8_A_PLANE];
-  unsigned char B[I8_STAGES][I8_B_STAGE];  // plane stride n_rows * 32 of the stage's tile
+  unsigned char B[I8_STAGES][I8_B_SLOT];  // planes 0..4 (32 rows each), then a zero plane
   double partial[2][4][I8_M];              // upper column half's per-point sums
   unsigned long long full[I8_STAGES];
   unsigned long long empty[I8_STAGES];
@@ -328,8 +329,10 @@ out:
     if (!mbar_wait_quiet(&S.full[f % I8_STAGES], (f / I8_STAGES) & 1)) atomicOr(P.err, 4);
 }
 
-// Lane 0 of the MMA warp: per N tile, all K chunks' 15 digit products into
-// the six level accumulators of the tile's set (sets alternate by tile).
+// Lane 0 of the MMA warp: per N tile, all K chunks' 19 digit products into
+// the six level accumulators of the tile's set (sets alternate by tile), five
+// MMA instructions per stage (one ~50-cycle issue each, so that issuing no
+// longer outlasts the tensor work of a stage).
 __device__ void mma_role(const I8Params &P, I8Smem &S, uint32_t tmem) {
   volatile int *abort_flag = &S.abort_flag;
   uint32_t fill = 0, tile_ctr = 0;
@@ -338,8 +341,6 @@ __device__ void mma_role(const I8Params &P, I8Smem &S, uint32_t tmem) {
     const I8Item W = P.items[it];
     for (int t = 0; t < P.T; ++t)
       for (int jn = 0; jn < W.n_nt; ++jn, ++tile_ctr) {
-        const int N = tile_rows(W.nc, jn, W.n_nt);
-        const uint32_t idesc = idesc_n(N);
         const int set = tile_ctr & 1;
         const uint32_t dcol = tmem + (uint32_t)(set * I8_SET_COLS);
         if (!mbar_wait(&S.acc_empty[set], ((tile_ctr >> 1) & 1) ^ 1, abort_flag, P.err)) goto out;
@@ -348,23 +349,19 @@ __device__ void mma_role(const I8Params &P, I8Smem &S, uint32_t tmem) {
           const int st = fill % I8_STAGES;
           if (!mbar_wait(&S.full[st], (fill / I8_STAGES) & 1, abort_flag, P.err)) goto out;
           tc_fence_after();
-          uint64_t a[I8_SLICES], b[I8_SLICES];
+          // Digit levels along N: B planes 0..m of a stage are one contiguous
+          // matrix of 32 (m + 1) rows, so A plane s times planes 0..5-s, written
+          // from accumulator column 32 s on, puts product (s, u) into the
+          // columns of level s + u.  Plane s = 0 also multiplies the zero plane
+          // (rows 160..191), so its MMA covers all six levels and alone starts
+          // the accumulation of a tile; the other four always accumulate.
+          const uint64_t bdesc = smem_desc<I8_LBO, I8_SBO>(smem_u32(S.B[st]));
 #pragma unroll
           for (int s = 0; s < I8_SLICES; ++s) {
-            a[s] = smem_desc<I8_LBO, I8_SBO>(smem_u32(S.A[st][s]));
-            b[s] = smem_desc<I8_LBO, I8_SBO>(smem_u32(S.B[st]) + (uint32_t)(s * N * I8_ROWB));
+            const int n_mma = I8_N * (s == 0 ? I8_LEVELS : I8_LEVELS - s);  // 192, 160, 128, 96, 64
+            umma_i8(dcol + (uint32_t)(s * I8_N), smem_desc<I8_LBO, I8_SBO>(smem_u32(S.A[st][s])), bdesc,
+                    idesc_n(n_mma), (s > 0 || kc > 0) ? 1u : 0u);
           }
-          uint32_t first[I8_LEVELS];
-#pragma unroll
-          for (int l = 0; l < I8_LEVELS; ++l) first[l] = kc > 0 ? 1u : 0u;
-#pragma unroll
-          for (int s = 0; s < I8_SLICES; ++s)
-#pragma unroll
-            for (int u = 0; u < I8_SLICES; ++u)
-              if (s + u < I8_LEVELS) {
-                umma_i8(dcol + (uint32_t)((s + u) * I8_N), a[s], b[u], idesc, first[s + u]);
-                first[s + u] = 1u;
-              }
           umma_commit(&S.empty[st]);
           issued = true;
         }
@@ -535,6 +532,13 @@ __global__ void __launch_bounds__(I8_THREADS, 1) rho1_i8_kernel(const I8Params P
     S.abort_flag = 0;
     mbar_init_fence();
   }
+  // the zero B plane of every stage (never written by the copies), made
+  // visible to the tensor core's (async proxy) reads
+  for (int e = tid; e < I8_STAGES * I8_N * I8_ROWB / 16; e += I8_THREADS) {
+    const int st = e / (I8_N * I8_ROWB / 16), o = e % (I8_N * I8_ROWB / 16);
+    reinterpret_cast<uint4 *>(S.B[st] + I8_B_STAGE)[o] = make_uint4(0u, 0u, 0u, 0u);
+  }
+  fence_proxy_async_smem();
   if (warp == 0) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&S.tmem_base)),
                  "r"(I8_TMEM_COLS));
