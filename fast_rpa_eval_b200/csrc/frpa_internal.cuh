@@ -119,7 +119,7 @@ static_assert(sizeof(I8Item) == 80, "I8Item layout");
 // One N tile of one batch and perturbation, packed by one CTA.
 struct I8BTile {
   int ib_off, nc, jn, t;
-  int n_rows, n_kc, sb_off, pad_;  // rows of this tile (multiple of 16, <= 32)
+  int n_rows, n_kc, sb_off, pad_;  // rows of this tile (32; rows past n_compute are zero)
   long long b_off;                 // bytes of the tile's first chunk
 };
 static_assert(sizeof(I8BTile) == 40, "I8BTile layout");

@@ -25,9 +25,9 @@
 //      per-point scales and writes phi's five digit planes in the tcgen05
 //      shared-memory tile image (K-major, no swizzle, 8 x 16-byte core
 //      matrices), one 32-wide K chunk after another, 16 points at a time;
-//   2. pack B: one CTA per (batch, perturbation, N tile of <= 32 rows)
-//      gathers P1c = P1[ib, ib] (lanes along P1's contiguous rows) and writes
-//      its digit planes the same way;
+//   2. pack B: one CTA per (batch, perturbation, N tile of 32 rows, the last
+//      one zero-padded) gathers P1c = P1[ib, ib] (lanes along P1's contiguous
+//      rows) and writes its digit planes the same way;
 //   3. contract: one persistent CTA per SM.  A loader thread moves each
 //      stage's A and B chunks into a 4-stage shared-memory ring with bulk
 //      copies; an MMA thread issues a stage's 19 digit products as five
