@@ -104,7 +104,7 @@ static_assert(sizeof(Rho1WorkItem) == 40, "work item layout");
 // in turn, so the scratch holds one group at a time.
 struct I8Item {
   int batch, nc, p0, pn;
-  int prefix, rows8, n_nt, n_kc;  // rows8 = pn rounded up to 8; N tiles of <= 96 rows; K chunks of 32
+  int prefix, rows8, n_nt, n_kc;  // rows8 = pn rounded up to 8; N tiles of 32 rows; K chunks of 32
   long long wave_off;
   long long a_off;       // bytes of the item's first A chunk
   long long b_off;       // bytes of the batch's first B chunk (t = 0)
