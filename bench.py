@@ -613,6 +613,16 @@ def run_frpa(args, ranks: Ranks):
                                    "(no FP64 figure in MEASURED_PEAKS.json)",
                     "algorithmic_flops_per_launch": w_flops,
                     "hbm_frac_of_measured": (w_bytes / (ms_fp64 / 1e3) / 1e9) / peaks["hbm_gbs"]}
+    elif mode == _lib.RHO1_SPLIT_I8:
+        traffic = profile_traffic("rho1_split_i8_step")
+        gbs = traffic / (ms / 1e3) / 1e9 if traffic else w_bytes / (ms / 1e3) / 1e9
+        roofline = {"bound": "hbm", "achieved": gbs, "peak": peaks["hbm_gbs"], "unit": "GB/s",
+                    "frac": gbs / peaks["hbm_gbs"], "traffic": traffic,
+                    "kernel": "split-int8 step (i8_pack_a_kernel, i8_pack_b_kernel, rho1_i8_kernel per group)",
+                    "achieved_from": "measured DRAM bytes per step (profiles/traffic.json) over the CUDA-event time",
+                    "peak_source": peaks["source"] + " (MEASURED_PEAKS.json hbm_gbs)",
+                    "algorithmic_bytes_per_launch": w_bytes,
+                    "algorithmic_hbm_frac": w_bytes / (ms / 1e3) / 1e9 / peaks["hbm_gbs"]}
     else:
         gbs = w_bytes / (ms / 1e3) / 1e9
         roofline = {"bound": "hbm", "achieved": gbs, "peak": peaks["hbm_gbs"], "unit": "GB/s",
@@ -624,12 +634,18 @@ def run_frpa(args, ranks: Ranks):
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-        "dtype": "f64" if mode == _lib.RHO1_FP64 else "f64 in/out, bf16x5 slices -> f32 (tcgen05) contraction",
+        "dtype": {_lib.RHO1_FP64: "f64",
+                  _lib.RHO1_SPLIT_BF16: "f64 in/out, bf16x5 slices -> f32 (tcgen05) contraction",
+                  _lib.RHO1_SPLIT_I8: "f64 in/out, int8x5 digit planes -> exact int32 level sums (tcgen05 kind::i8) "
+                                      "contraction, f64 recombination and ddots"}[mode],
         "data": "synthetic (seeded config-2 recipe: Gaussian x Y_lm basis, phi generated on the GPU)",
         "config": {"workload": "config2: rho1 + grad rho1, 1000 atoms at 0.1/A^3, 10 functions/atom, "
                                f"{p.n_my_batches_work} batches of 100-300 points, n_compute 100-600, T=1",
                    "path": mode_name, "valid_batches": info["n_valid_batches"], "work_items": n_items_tuned,
-                   "launch": "one persistent grouped launch per step, replayed from a CUDA graph",
+                   "launch": ("one persistent grouped launch per step, replayed from a CUDA graph"
+                              if mode != _lib.RHO1_SPLIT_I8 else
+                              f"row max + {i8_groups} groups x (pack phi, pack P1c, contraction), "
+                              "replayed from a CUDA graph"),
                    "tuning": tuned or "defaults (--no-tune)",
                    "grid_points_per_rank": w_points,
                    "l2": "inputs larger than L2 (phi + grad phi = %.1f GB per rank)" % (4 * 8 * p.wave_len / 1e9),
