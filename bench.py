@@ -194,12 +194,15 @@ def measured_peaks():
     return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "bf16_tflops_sustained": 1400.0, "source": "fallback"}
 
 
-def profile_traffic(name: str):
-    """DRAM bytes per launch from the committed ncu summary, if present."""
+def profile_traffic(name: str, batches: int = 30_000):
+    """DRAM bytes of one step from the committed ncu summary, if present; the
+    figures are for the 30,000-batch config-2 step and are scaled to
+    `batches` (traffic grows with the batch count)."""
     path = os.path.join(ROOT, "profiles", "traffic.json")
     if os.path.exists(path):
         with open(path) as f:
-            return json.load(f).get(name)
+            v = json.load(f).get(name)
+        return None if v is None else v * batches / 30_000
     return None
 
 
@@ -499,7 +502,7 @@ def run_frpa(args, ranks: Ranks):
                               "hbm_gbs_algorithmic": w_bytes / (ms_split / 1e3) / 1e9,
                               "frac_of_measured_hbm": w_bytes / (ms_split / 1e3) / 1e9 / peaks["hbm_gbs"],
                               "bf16_equivalent_tflops": 15 * w_flops / (ms_split / 1e3) / 1e12}
-    i8_traffic = profile_traffic("rho1_split_i8_step")
+    i8_traffic = profile_traffic("rho1_split_i8_step", p.n_my_batches_work)
     out["rho1_split_i8"] = {
         "pts_per_s": total_pts / (ms_i8 / 1e3), "ms_per_step": ms_i8, "speedup_vs_fp64": ms_fp64 / ms_i8,
         "kernels_per_group": "pack A (phi digits), pack B (P1c digits), tcgen05.mma.kind::i8 contraction",
@@ -607,14 +610,14 @@ def run_frpa(args, ranks: Ranks):
 
     if mode == _lib.RHO1_FP64:
         roofline = {"bound": "tensor", "achieved": achieved_tf, "peak": fp64_peak, "unit": "TFLOP/s",
-                    "frac": achieved_tf / fp64_peak, "traffic": profile_traffic("rho1_fp64_kernel"),
+                    "frac": achieved_tf / fp64_peak, "traffic": profile_traffic("rho1_fp64_kernel", p.n_my_batches_work),
                     "kernel": "rho1_fp64_kernel",
                     "peak_source": "measured on this GPU in this run: FP64 m8n8k4 MMA throughput probe "
                                    "(no FP64 figure in MEASURED_PEAKS.json)",
                     "algorithmic_flops_per_launch": w_flops,
                     "hbm_frac_of_measured": (w_bytes / (ms_fp64 / 1e3) / 1e9) / peaks["hbm_gbs"]}
     elif mode == _lib.RHO1_SPLIT_I8:
-        traffic = profile_traffic("rho1_split_i8_step")
+        traffic = profile_traffic("rho1_split_i8_step", p.n_my_batches_work)
         gbs = traffic / (ms / 1e3) / 1e9 if traffic else w_bytes / (ms / 1e3) / 1e9
         roofline = {"bound": "hbm", "achieved": gbs, "peak": peaks["hbm_gbs"], "unit": "GB/s",
                     "frac": gbs / peaks["hbm_gbs"], "traffic": traffic,
@@ -626,7 +629,7 @@ def run_frpa(args, ranks: Ranks):
     else:
         gbs = w_bytes / (ms / 1e3) / 1e9
         roofline = {"bound": "hbm", "achieved": gbs, "peak": peaks["hbm_gbs"], "unit": "GB/s",
-                    "frac": gbs / peaks["hbm_gbs"], "traffic": profile_traffic("rho1_split_kernel"),
+                    "frac": gbs / peaks["hbm_gbs"], "traffic": profile_traffic("rho1_split_kernel", p.n_my_batches_work),
                     "kernel": "rho1_split_kernel", "peak_source": peaks["source"] + " (MEASURED_PEAKS.json hbm_gbs)",
                     "algorithmic_bytes_per_launch": w_bytes,
                     "bf16_equivalent_tflops": 15 * w_flops / (ms / 1e3) / 1e12,
