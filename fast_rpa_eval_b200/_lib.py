@@ -387,9 +387,13 @@ class Session:
     init_dfpt_device_data, the *_cu_host_ twins, free_*.  Holds references to
     every host array passed in so they outlive the calls."""
 
-    def __init__(self, rho_prob, sumup_prob=None, wave=None, gradient_wave=None):
+    def __init__(self, rho_prob, sumup_prob=None, wave=None, gradient_wave=None, entry=None):
         """``wave`` / ``gradient_wave`` (device tensors) replace the problem's
-        host arrays; the session then uses them in place."""
+        host arrays; the session then uses them in place.  ``entry``: an object
+        whose attributes replace the library's entry points of the same names
+        (e.g. callables that reach the C++-linkage exports the way the
+        reference's C++ callers bind them); default: the C-linkage exports."""
+        self._entry = entry
         self.rho_prob, self.sumup_prob = rho_prob, sumup_prob
         T = rho_prob.T
         if sumup_prob is not None and sumup_prob.T != T:
@@ -397,7 +401,7 @@ class Session:
         set_atom_tile_size(T)
         L = lib()
         L.frpa_clear_error()
-        L.init_dfpt_device_info()
+        self._fn("init_dfpt_device_info")()
         check_void_call()
         k = self._k = _Keep()
         r, s = rho_prob, sumup_prob
@@ -416,7 +420,7 @@ class Session:
         g = (lambda name, kind: (k.i if kind == "i" else k.d)(getattr(s, name)) if s is not None else
              (k.i(zi) if kind == "i" else k.d(z)))
         dm = r.density_matrix if r.density_matrix is not None else np.zeros(1)
-        L.init_dfpt_device_data(
+        self._fn("init_dfpt_device_data")(
             _iref(r.n_my_batches_work), _iref(r.n_full_points), _iref(sc["n_valid"]), _iref(r.n_basis),
             _iref(sc["n_atoms"]), _iref(r.n_max_compute_ham), _iref(r.n_centers_basis_I), _iref(r.n_max_batch_size),
             _iref(sc["l_pot_max"]), _iref(sc["n_max_radial"]), _iref(sc["n_hartree_grid"]), _iref(sc["n_centers"]),
@@ -468,7 +472,7 @@ class Session:
         zi = np.zeros(1, np.int32)
         z = np.zeros(1)
         lib().frpa_clear_error()
-        fn = lib().sum_up_whole_potential_c_v3_atoms_full_points_j_atom_tile_cu_host_
+        fn = self._fn("sum_up_whole_potential_c_v3_atoms_full_points_j_atom_tile_cu_host_")
         fn(c_int(s.j_atom_begin), c_int(s.j_atom_end), c_int(s.n_full_points), c_int(s.l_max_analytic_multipole),
            c_int(s.index_cc_dim_0), c_int(s.n_valid_points), c_int(s.l_pot_max), c_int(s.n_max_radial),
            c_int(s.n_hartree_grid), c_int(s.n_centers), c_int(s.n_centers_hartree_potential), c_int(s.n_atoms),
@@ -481,10 +485,13 @@ class Session:
         check_void_call()
         return dv.reshape((s.n_full_points, s.T), order="F")
 
+    def _fn(self, name):
+        f = getattr(self._entry, name, None) if self._entry is not None else None
+        return f if f is not None else getattr(lib(), name)
+
     def close(self):
-        L = lib()
-        L.free_dfpt_device_data()
-        L.free_dfpt_device_info()
+        self._fn("free_dfpt_device_data")()
+        self._fn("free_dfpt_device_info")()
 
     def __enter__(self):
         return self

@@ -110,12 +110,12 @@ int rho1_bias_part2_launch(const Rho1Plan &plan, const int *h_atom_valid, const 
       }
   }
   if (plan.n_items == 0) return FRPA_OK;
-  static int configured[64] = {0};
-  if (plan.device >= 0 && plan.device < 64 && !configured[plan.device]) {
+  static PerDeviceOnce configured;
+  FRPA_TRY(configured.run(plan.device, []() -> int {
     FRPA_CUDA_TRY(
         cudaFuncSetAttribute(bias_part2_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(BiasSmem)));
-    configured[plan.device] = 1;
-  }
+    return FRPA_OK;
+  }));
   bias_part2_kernel<<<plan.n_items, BZ_THREADS, sizeof(BiasSmem), stream>>>(
       plan.d_items, plan.d_ib, d_atom_valid, n_atoms, j_atom_begin, n_active, j_coord, plan.n_basis,
       plan.n_max_batch_size, plan.n_batches, wave, gwave, dm, bias, plan.d_err);

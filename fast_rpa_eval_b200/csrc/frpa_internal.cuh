@@ -6,6 +6,7 @@
 #include <cstdarg>
 #include <cstdint>
 #include <cstdio>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -42,6 +43,25 @@ void clear_error();
 // Launch-time check: configuration errors surface here, execution errors at
 // the next synchronising call.
 #define FRPA_LAUNCH_CHECK() FRPA_CUDA_TRY(cudaGetLastError())
+
+// One-time setup per device (kernel attributes, constant-memory uploads) that
+// several host threads may reach at the same time: `fn` runs under a lock and
+// is retried by the next caller until it has succeeded once for `device`.
+class PerDeviceOnce {
+ public:
+  template <class F>
+  int run(int device, F &&fn) {
+    std::lock_guard<std::mutex> lk(mu_);
+    if (device >= 0 && device < 64 && done_[device]) return FRPA_OK;
+    const int st = fn();
+    if (st == FRPA_OK && device >= 0 && device < 64) done_[device] = true;
+    return st;
+  }
+
+ private:
+  std::mutex mu_;
+  bool done_[64] = {};
+};
 
 // ------------------------------------------------------------ device math --
 

@@ -605,12 +605,12 @@ int rho1_split_launch(const Rho1Plan &plan, int n_active, const double *wave, co
       grad, 0, sizeof(double) * 3 * (size_t)plan.n_max_batch_size * plan.n_batches * plan.T, stream));
   if (plan.n_items_split == 0) return FRPA_OK;
   FRPA_TRY(p1_rowmax_launch(plan, P1, stream));
-  static int configured[64] = {0};
+  static PerDeviceOnce configured;
   const int smem = rho1_split_smem_bytes();
-  if (plan.device >= 0 && plan.device < 64 && !configured[plan.device]) {
+  FRPA_TRY(configured.run(plan.device, [smem]() -> int {
     FRPA_CUDA_TRY(cudaFuncSetAttribute(rho1_split_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-    configured[plan.device] = 1;
-  }
+    return FRPA_OK;
+  }));
   int n_sm = 148;
   FRPA_CUDA_TRY(cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, plan.device));
   SplitParams P;

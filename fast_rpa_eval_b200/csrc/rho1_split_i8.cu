@@ -740,12 +740,12 @@ int rho1_i8_launch(Rho1Plan &plan, int n_active, const double *wave, const doubl
   if (plan.i8_groups.empty()) return FRPA_OK;
   FRPA_TRY(i8_scratch(plan, stream));
   FRPA_TRY(p1_rowmax_launch(plan, P1, stream));
-  static int configured[64] = {0};
+  static PerDeviceOnce configured;
   const int smem = i8_smem_bytes();
-  if (plan.device >= 0 && plan.device < 64 && !configured[plan.device]) {
+  FRPA_TRY(configured.run(plan.device, [smem]() -> int {
     FRPA_CUDA_TRY(cudaFuncSetAttribute(rho1_i8_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-    configured[plan.device] = 1;
-  }
+    return FRPA_OK;
+  }));
   int n_sm = 148;
   FRPA_CUDA_TRY(cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, plan.device));
   I8Params P;

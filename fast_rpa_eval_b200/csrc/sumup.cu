@@ -571,9 +571,7 @@ static int upload(void **dst, const void *src, size_t bytes) {
   return FRPA_OK;
 }
 
-int sumup_upload_constants(int device) {
-  static bool done[64] = {false};
-  if (device >= 0 && device < 64 && done[device]) return FRPA_OK;
+static int sumup_upload_constants_once() {
   double K[SU_LMAX + 1][SU_LMAX + 1] = {}, Kc[SU_LMAX + 1][SU_LMAX + 1] = {};
   double RA[SU_LMAX + 1][SU_LMAX + 1] = {}, RB[SU_LMAX + 1][SU_LMAX + 1] = {}, DF[SU_LMAX + 1] = {};
   const double four_pi = 12.566370614359172953850573533118;
@@ -610,8 +608,14 @@ int sumup_upload_constants(int device) {
         kabc[2][k] = c;
       }
   FRPA_CUDA_TRY(cudaMemcpyToSymbol(c_kabc, kabc, sizeof(kabc)));
-  if (device >= 0 && device < 64) done[device] = true;
   return FRPA_OK;
+}
+
+// The constant tables, uploaded once per device (plan creation and the
+// allocation-free entry point may reach this from several host threads).
+int sumup_upload_constants(int device) {
+  static PerDeviceOnce uploaded;
+  return uploaded.run(device, sumup_upload_constants_once);
 }
 
 void sumup_plan_free(SumupPlan *P) {
@@ -955,6 +959,12 @@ int noalloc_scratch_address(int device, unsigned char **out) {
     if (e != cudaSuccess)
       return fail(FRPA_ERR_CUDA, "noalloc sum-up: cudaGetSymbolAddress failed: %s", cudaGetErrorString(e));
     FRPA_TRY(sumup_upload_constants(device));
+    // the input-flag word at the start of the array collects the flags of
+    // every call on this device until frpa_sumup_noalloc_flags reads it
+    e = cudaMemset(p, 0, sizeof(int));
+    if (e == cudaSuccess) e = cudaDeviceSynchronize();
+    if (e != cudaSuccess)
+      return fail(FRPA_ERR_CUDA, "noalloc sum-up: clearing the flag word failed: %s", cudaGetErrorString(e));
     g_noalloc_addr[device] = p;
   }
   *out = static_cast<unsigned char *>(g_noalloc_addr[device]);
@@ -1014,8 +1024,9 @@ extern "C" int frpa_sumup_execute_noalloc(
   double *mc = reinterpret_cast<double *>(base + flag_bytes + table_bytes);
   const int L2 = (L + 1) * (L + 1);
   // every scratch word read below is written first in this call, so nothing
-  // left by an earlier call is used; the flag is cleared explicitly
-  FRPA_CUDA_TRY(cudaMemsetAsync(err, 0, sizeof(int), stream));
+  // left by an earlier call is used; the flag word (bit 0: an
+  // l_hartree_max_far_distance entry outside 0..l_pot_max, clamped) keeps
+  // collecting until frpa_sumup_noalloc_flags reads and clears it
   noalloc_pack_table_kernel<<<(index_cc_dim_0 + 255) / 256, 256, 0, stream>>>(index_cc_dim_0, index_cc_dim_0,
                                                                                index_cc, packed);
   FRPA_LAUNCH_CHECK();
@@ -1031,5 +1042,22 @@ extern "C" int frpa_sumup_execute_noalloc(
       multipole_radius_sq, outer_potential_radius, n_cc_lm_ijk, packed, index_ijk_max_cc, index_cc_dim_0, mc, spline,
       delta_v_hartree, nullptr);
   FRPA_LAUNCH_CHECK();
+  return FRPA_OK;
+}
+
+extern "C" int frpa_sumup_noalloc_flags(int *flags, void *stream_) {
+  using namespace frpa;
+  clear_error();
+  FRPA_CHECK_ARG(flags != nullptr, "noalloc sum-up flags: null output");
+  int device = 0;
+  FRPA_CUDA_TRY(cudaGetDevice(&device));
+  unsigned char *base = nullptr;
+  FRPA_TRY(noalloc_scratch_address(device, &base));
+  cudaStream_t stream = (cudaStream_t)stream_;
+  int v = 0;
+  FRPA_CUDA_TRY(cudaMemcpyAsync(&v, base, sizeof(int), cudaMemcpyDeviceToHost, stream));
+  FRPA_CUDA_TRY(cudaMemsetAsync(base, 0, sizeof(int), stream));
+  FRPA_CUDA_TRY(cudaStreamSynchronize(stream));
+  *flags = v;
   return FRPA_OK;
 }

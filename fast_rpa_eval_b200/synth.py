@@ -405,6 +405,31 @@ def make_rho1_problem(
     )
 
 
+def first_order_h_inputs(prob: Rho1Problem, seed: int = 7, pad_value: float = 0.0) -> dict:
+    """Seeded stand-ins for the exchange-correlation inputs of the first-order
+    H integration (evaluate_first_order_H.cpp:13-53), in the reference's
+    layouts: vsigma (3, nmb, nb), gradient_rho (3, n_full), hessian_wave
+    (6 wave_len, rows past n_compute set to pad_value), H_prefactor1
+    (nmb, nb, T), first_order_gradient_rho (3, nmb, nb, T), first_order_rho
+    (n_full, T), v2rho2 (3, nmb, nb), v2rhosigma (6, nmb, nb), v2sigma2
+    (6, nmb, nb).  Only their values matter for parity, so they are drawn
+    N(0, 1) with mild scales rather than from a functional."""
+    rng = np.random.default_rng(seed)
+    nb, nmb, nf, T = prob.n_my_batches_work, prob.n_max_batch_size, prob.n_full_points, prob.T
+    hess = rng.normal(size=6 * prob.wave_len)
+    for b in range(nb):  # the padding rows of every (component, point) column
+        nc, npb = int(prob.n_compute_c_batches[b]), int(prob.n_point_batches[b])
+        ncp = (nc + 3) // 4 * 4
+        if nc > 0 and ncp > nc:
+            blk = hess[6 * int(prob.i_batch_2_wave_offset[b]):][: 6 * ncp * npb].reshape((ncp, 6 * npb), order="F")
+            blk[nc:, :] = pad_value
+    f = lambda *shape: np.asfortranarray(rng.normal(size=shape))  # noqa: E731
+    return dict(vsigma=0.5 * f(3, nmb, nb), gradient_rho=f(3, nf), hessian_wave=hess,
+                H_prefactor1=f(nmb, nb, T), first_order_gradient_rho=f(3, nmb, nb, T),
+                first_order_rho=f(nf, T), v2rho2=0.3 * f(3, nmb, nb), v2rhosigma=0.2 * f(6, nmb, nb),
+                v2sigma2=0.1 * f(6, nmb, nb))
+
+
 def config1(seed: int = 1, **kw) -> Rho1Problem:
     """Benchmark config 1: the CPU-runnable plain FP64 case."""
     return make_rho1_problem(seed=seed, **kw)

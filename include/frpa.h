@@ -123,12 +123,33 @@ void sum_up_whole_potential_c_v3_atoms_full_points_j_atom_tile_(
     double *delta_v_hartree);
 
 /* Replaces sum_up_whole_potential_c_v3_atoms_full_points_j_atom_tile_cu_host_
- * (sum_up_whole_potential.h:50-95, sum_up_whole_potential.cu:548-769; C++
- * linkage there, C linkage here).  Scalars by value.  Constant arrays come from
- * the session; the changeable ones (l_hartree_max_far_distance,
- * multipole_radius_sq, outer_potential_radius, multipole_moments, the spline
- * table and delta_v_hartree) are uploaded from the host pointers, and
- * delta_v_hartree is downloaded again (sum_up_whole_potential.cu:641-647,768-769). */
+ * (sum_up_whole_potential.h:50-95, sum_up_whole_potential.cu:548-769).
+ * Scalars by value.  Constant arrays come from the session; the changeable
+ * ones (l_hartree_max_far_distance, multipole_radius_sq, outer_potential_radius,
+ * multipole_moments, the spline table and delta_v_hartree) are uploaded from
+ * the host pointers, and delta_v_hartree is downloaded again
+ * (sum_up_whole_potential.cu:641-647,768-769).
+ * The reference gives this entry point C++ linkage.  The library exports it
+ * twice: C++ code that includes this header (or the reference's own
+ * sum_up_whole_potential.h) binds the C++-linkage symbol, as the reference's
+ * C++ callers do, unmodified; C and Fortran callers bind the same function
+ * under C linkage. */
+#ifdef __cplusplus
+} /* extern "C" */
+void sum_up_whole_potential_c_v3_atoms_full_points_j_atom_tile_cu_host_(
+    const int j_atom_begin, const int j_atom_end, const int n_full_points, const int l_max_analytic_multipole,
+    const int index_cc_dim_0, const int n_valid_points, const int l_pot_max, const int n_max_radial,
+    const int n_hartree_grid, const int n_centers, const int n_centers_hartree_potential, const int n_atoms,
+    const int hartree_force_l_add, const int n_species, const int *n_radial, const int *species,
+    const int *species_center, const int *l_hartree_max_far_distance, const int *i_valid_point_2_i_full_points_map,
+    const double *coord_points, const double *multipole_radius_sq, const double *outer_potential_radius,
+    const double *multipole_moments, const double *current_delta_v_hart_part_spl_tile, const int *l_hartree,
+    const int *n_grid, const int *n_cc_lm_ijk, const int *centers_hartree_potential, const int *center_to_atom,
+    const int *index_cc, const int *index_ijk_max_cc, const double *cc, const double *coords_center,
+    const double *r_grid_min, const double *log_r_grid_inc, const double *scale_radial, const double *partition_tab,
+    double *delta_v_hartree);
+extern "C" {
+#else
 void sum_up_whole_potential_c_v3_atoms_full_points_j_atom_tile_cu_host_(
     int j_atom_begin, int j_atom_end, int n_full_points, int l_max_analytic_multipole, int index_cc_dim_0,
     int n_valid_points, int l_pot_max, int n_max_radial, int n_hartree_grid, int n_centers,
@@ -141,6 +162,7 @@ void sum_up_whole_potential_c_v3_atoms_full_points_j_atom_tile_cu_host_(
     const int *index_ijk_max_cc, const double *cc, const double *coords_center, const double *r_grid_min,
     const double *log_r_grid_inc, const double *scale_radial, const double *partition_tab,
     double *delta_v_hartree);
+#endif
 
 /* Replaces generate_first_order_rho_bias_part2_
  * (generate_first_order_rho_bias_part2.cpp:11-168): the density-matrix part
@@ -157,18 +179,26 @@ void generate_first_order_rho_bias_part2_(
     int *i_batch_2_wave_offset, double *wave_batches_compress, double *gradient_wave_batches_compress,
     double *first_order_rho_bias_part2, double *partition_tab, double *density_matrix);
 
-/* Replaces init_dfpt_device_info (device.hpp:191, device.cu:7-33): selects
- * device 0 (or $FRPA_DEVICE) and creates the session stream. */
+/* The reference's device session.  The reference declares these four with
+ * C++ linkage (device.hpp:191-192, device_data.hpp:159-227); as for the sum-up
+ * cu_host_ entry point above, C++ code including this header binds the
+ * C++-linkage symbols, C and Fortran code the C-linkage ones (both exported).
+ *
+ * init_dfpt_device_info replaces device.cu:7-33: selects device 0 (or
+ * $FRPA_DEVICE) and creates the session stream.  free_dfpt_device_info
+ * replaces device.cu:35-38.
+ *
+ * init_dfpt_device_data replaces device_data.cu:10-361: validates and uploads
+ * the constant arrays once, builds the rho1 work list (the reference's
+ * valid-batch list and per-tile GEMM metadata, device_data.cu:242-300) and the
+ * sum-up plan.  Wave arrays that are already device memory of the session's
+ * GPU are used in place (not copied); the caller keeps them alive until
+ * free_dfpt_device_data (device_data.cu:363-431). */
+#ifdef __cplusplus
+} /* extern "C" */
+#endif
 void init_dfpt_device_info(void);
-/* Replaces free_dfpt_device_info (device.hpp:192, device.cu:35-38). */
 void free_dfpt_device_info(void);
-
-/* Replaces init_dfpt_device_data (device_data.hpp:159-225, device_data.cu:10-361):
- * validates and uploads the constant arrays once, builds the rho1 work list
- * (the reference's valid-batch list and per-tile GEMM metadata,
- * device_data.cu:242-300) and the sum-up plan.  Wave arrays that are already
- * device memory of the session's GPU are used in place (not copied); the
- * caller keeps them alive until free_dfpt_device_data. */
 void init_dfpt_device_data(
     int *n_my_batches_work, int *n_full_points, int *n_valid_points, int *n_basis, int *n_atoms,
     int *n_max_compute_ham, int *n_centers_basis_I, int *n_max_batch_size, int *l_pot_max, int *n_max_radial,
@@ -184,9 +214,10 @@ void init_dfpt_device_data(
     double *first_order_gradient_rho, double *first_order_gradient_rho_bias_batches_atoms,
     int *l_hartree_max_far_distance, double *multipole_radius_sq, double *outer_potential_radius,
     double *multipole_moments, double *current_delta_v_hart_part_spl_tile, double *delta_v_hartree);
-
-/* Replaces free_dfpt_device_data (device_data.hpp:227, device_data.cu:363-431). */
 void free_dfpt_device_data(void);
+#ifdef __cplusplus
+extern "C" {
+#endif
 
 /* Device addresses of the session's resident rho1 outputs (after a
  * *_cu_host_ call), for callers that keep working on the GPU. */
@@ -351,6 +382,13 @@ int frpa_sumup_execute_noalloc(
 /* Reads and clears the device-side input flags of the last executions
  * (bit 0: an l_hartree_max_far_distance entry outside 0..l_pot_max, clamped). */
 int frpa_sumup_device_flags(const frpa_sumup_plan *plan, int *flags);
+
+/* The same input flags for frpa_sumup_execute_noalloc on the current device:
+ * every call of that entry point ORs into one flag word inside the library
+ * (bit 0: an l_hartree_max_far_distance entry outside 0..l_pot_max was
+ * clamped); this reads it after the work queued on `stream`, clears it and
+ * waits for the stream.  Allocates nothing.  No counterpart in the reference. */
+int frpa_sumup_noalloc_flags(int *flags, void *stream);
 
 /* =========================================================================
  * Synthetic workload generator (benchmarks and tests)

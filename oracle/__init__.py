@@ -31,16 +31,22 @@ c_dbl_p = ctypes.POINTER(ctypes.c_double)
 c_u8_p = ctypes.POINTER(ctypes.c_ubyte)
 
 
+def reference_tree() -> str:
+    """The reference checkout: $FR_REF, else the directory `reference` beside
+    this repository (the layout the build container has)."""
+    return os.environ.get("FR_REF") or os.path.join(os.path.dirname(os.path.dirname(_HERE)), "reference")
+
+
 def build(with_reference: bool | None = None) -> None:
     """Compile liboracle.so (and the reference libraries where the reference
     tree is present)."""
     targets = ["oracle"]
-    ref = os.environ.get("FR_REF", "/root/reference")
+    ref = reference_tree()
     if with_reference is None:
         with_reference = os.path.isdir(os.path.join(ref, "fast_rap_src_dfpt_gpu_eval"))
     if with_reference:
         targets.append("ref")
-    subprocess.run(["make", "-s", "-C", _HERE] + targets, check=True)
+    subprocess.run(["make", "-s", "-C", _HERE, "FR_REF=" + os.path.abspath(ref)] + targets, check=True)
 
 
 def _load(name: str):
@@ -210,38 +216,55 @@ def far_field_spherical(l_max: int, points_3xn, atoms_3xn, Q_lm_by_atom):
 # --------------------------------------------------------------------------
 
 
-def first_order_h(prob, v, use_reference: bool = False, w=None):
-    """H (n_basis, n_basis, T) = sum_p w v phi_i phi_j (accumulated from 0).
-    ``v`` is (n_full_points, T); ``w`` defaults to prob.partition_tab."""
+def first_order_h(prob, v, use_reference: bool = False, w=None, xc=None, j_coord: int | None = None):
+    """H (n_basis, n_basis, T) accumulated from 0 by the first-order-H
+    integration (evaluate_first_order_H.cpp:13-222).  ``v`` is
+    v_hartree_gradient (n_full_points, T); ``w`` defaults to
+    prob.partition_tab.  ``xc`` (optional) holds the other inputs in the
+    reference's layouts: vsigma (3, nmb, nb), gradient_rho (3, n_full),
+    hessian_wave (6 wave_len), H_prefactor1 (nmb, nb, T),
+    first_order_gradient_rho (3, nmb, nb, T), first_order_rho (n_full, T),
+    v2rho2 (3, nmb, nb), v2rhosigma (6, nmb, nb), v2sigma2 (6, nmb, nb);
+    absent ones are zero."""
     T = prob.T
     w = prob.partition_tab if w is None else w
+    jc = prob.j_coord if j_coord is None else j_coord
+    nb, nmb, nfull = prob.n_my_batches_work, prob.n_max_batch_size, prob.n_full_points
+    xc = dict(xc or {})
+    shapes = dict(vsigma=3 * nmb * nb, gradient_rho=3 * nfull, hessian_wave=6 * prob.wave_len,
+                  H_prefactor1=nmb * nb * T, first_order_gradient_rho=3 * nmb * nb * T, first_order_rho=nfull * T,
+                  v2rho2=3 * nmb * nb, v2rhosigma=6 * nmb * nb, v2sigma2=6 * nmb * nb)
+    arr = {k: (np.asarray(xc[k], dtype=np.float64).ravel(order="F") if k in xc else np.zeros(max(1, n)))
+           for k, n in shapes.items()}
     H = np.zeros(prob.n_basis * prob.n_basis * T)
     A = _Args()
     if not use_reference:
         lib = _load("liboracle.so")
         lib.oracle_first_order_h(
-            c_int(T), c_int(prob.n_my_batches_work), c_int(prob.j_atom_begin), c_int(prob.j_atom_end),
-            c_int(prob.n_full_points), c_int(prob.n_basis), c_int(prob.n_centers_basis_I),
-            A.i(prob.n_point_batches), A.i(prob.n_point_batches_prefix_sum),
-            A.i(prob.i_valid_point_2_i_full_points_map), A.i(prob.n_compute_c_batches), A.i(prob.i_basis_batches),
-            A.i(prob.i_batch_2_wave_offset), A.d(prob.wave), A.d(w), A.d(v), H.ctypes.data_as(c_dbl_p))
+            c_int(T), c_int(nb), c_int(prob.j_atom_begin), c_int(prob.j_atom_end), c_int(nfull), c_int(jc),
+            c_int(prob.n_basis), c_int(nmb), c_int(prob.n_centers_basis_I), A.i(prob.n_point_batches),
+            A.i(prob.n_compute_c_batches), A.i(prob.i_basis_batches), A.i(prob.atom_valid_n_compute_c_batches),
+            c_int(prob.n_atoms), A.i(prob.n_point_batches_prefix_sum), A.i(prob.i_valid_point_2_i_full_points_map),
+            A.d(arr["vsigma"]), A.d(arr["gradient_rho"]), A.i(prob.i_batch_2_wave_offset), A.d(prob.wave),
+            A.d(prob.gradient_wave), A.d(arr["hessian_wave"]), A.d(arr["H_prefactor1"]),
+            A.d(arr["first_order_gradient_rho"]), A.d(v), A.d(arr["first_order_rho"]), A.d(arr["v2rho2"]),
+            A.d(arr["v2rhosigma"]), A.d(arr["v2sigma2"]), A.d(w), H.ctypes.data_as(c_dbl_p))
     else:
         lib = _load(os.path.join("_ref", f"libref_t{T}.so"))
-        nb, nmb = prob.n_my_batches_work, prob.n_max_batch_size
-        z = lambda n: np.zeros(max(1, n))  # noqa: E731
-        ints = [prob.j_atom_begin, prob.j_atom_end, prob.n_full_points, prob.j_coord, prob.n_basis, prob.n_atoms,
+        ints = [prob.j_atom_begin, prob.j_atom_end, nfull, jc, prob.n_basis, prob.n_atoms,
                 prob.n_max_compute_ham, nmb, nb, prob.n_centers_basis_I]
         scal = [ctypes.byref(c_int(int(v_))) for v_ in ints]
         not_use = c_int(0)
+        z = lambda n: np.zeros(max(1, n))  # noqa: E731
         lib.evaluate_first_order_h_reduce_memory_c_v2_(
             *scal, A.i(prob.n_point_batches), A.i(prob.n_compute_c_batches), A.i(prob.i_basis_batches),
             A.i(prob.atom_valid_n_compute_c_batches), A.i(prob.n_point_batches_prefix_sum),
             A.i(prob.i_valid_point_2_i_full_points_map),
-            A.d(z(nmb * nb)), A.d(z(3 * nmb * nb)), A.d(z(3 * prob.n_full_points)),
+            A.d(z(nmb * nb)), A.d(arr["vsigma"]), A.d(arr["gradient_rho"]),
             A.d(z(prob.wave_len)), A.i(prob.i_batch_2_wave_offset), A.d(prob.wave), A.d(prob.gradient_wave),
-            A.d(z(6 * prob.wave_len)), H.ctypes.data_as(c_dbl_p), A.d(z(nmb * nb * T)), A.d(z(3 * nmb * nb * T)),
-            A.d(v), A.d(z(prob.n_full_points * T)), A.d(z(3 * nmb * nb)), A.d(z(6 * nmb * nb)),
-            A.d(z(6 * nmb * nb)), A.d(w), ctypes.byref(not_use))
+            A.d(arr["hessian_wave"]), H.ctypes.data_as(c_dbl_p), A.d(arr["H_prefactor1"]),
+            A.d(arr["first_order_gradient_rho"]), A.d(v), A.d(arr["first_order_rho"]), A.d(arr["v2rho2"]),
+            A.d(arr["v2rhosigma"]), A.d(arr["v2sigma2"]), A.d(w), ctypes.byref(not_use))
     return H.reshape((prob.n_basis, prob.n_basis, T), order="F")
 
 

@@ -326,46 +326,107 @@ void oracle_sumup(int T, int j_atom_begin, int j_atom_end, int n_full_points, in
 /* First-order H with zero XC terms: B/evaluate_first_order_H.cpp:13-222    */
 /* ------------------------------------------------------------------------ */
 
+/* First-order H with every term (evaluate_first_order_H.cpp:77-215).  Per
+ * batch and atom j of the tile (t = j - j_atom_begin), per point p:
+ *   lfos = 2 sum_k fogr(k, p) grad_rho(k, f)                       (:146-152)
+ *   pf2_k = 2 w(f) grad_rho(k, f) (v2rhosigma rho1 + v2sigma2 lfos)
+ *           + 2 w(f) vsigma fogr(k, p)                             (:153-160)
+ *   pf3 = w(f) (v_hartree_gradient + v2rho2 rho1 + v2rhosigma lfos) (:161-164)
+ *   pf5_k = 2 vsigma w(f) grad_rho(k, f)                           (:165-168)
+ *   cs1(i, p) = 0.5 (H_prefactor1 + pf3) phi_i + sum_k pf2_k dphi_i/dk (:170-178)
+ *              - sum_k pf5_k hess_i(k, j_coord) for i in atom j's range (:180-189)
+ * then H(ib_i, ib_j) += sum_p cs1(i, p) phi_j(p) + phi_i(p) cs1(j, p), the
+ * rank-2k update (:192-205) and its symmetric scatter (:207-215).  The XC
+ * arrays are indexed by their first component only, as the reference does
+ * (vsigma(0, p), v2rho2(0, p), v2rhosigma(0, p), v2sigma2(0, p)); vrho and
+ * H_times_psi are accepted and unused there as well. */
 void oracle_first_order_h(int T, int n_my_batches_work, int j_atom_begin, int j_atom_end, int n_full_points,
-                          int n_basis, int n_centers_basis_I, const int *n_point_batches,
-                          const int *n_point_batches_prefix_sum, const int *i_valid_point_2_i_full_points_map,
-                          const int *n_compute_c_batches, const int *i_basis_batches,
-                          const int *i_batch_2_wave_offset, const double *wave, const double *partition_tab,
-                          const double *v_hartree_gradient, double *first_order_H) {
-  int n_active = j_atom_end - j_atom_begin + 1;
-  if (n_active > T) n_active = T;
+                          int j_coord, int n_basis, int n_max_batch_size, int n_centers_basis_I,
+                          const int *n_point_batches, const int *n_compute_c_batches, const int *i_basis_batches,
+                          const int *atom_valid, int n_atoms, const int *n_point_batches_prefix_sum,
+                          const int *i_valid_point_2_i_full_points_map, const double *vsigma_batches,
+                          const double *gradient_rho, const int *i_batch_2_wave_offset, const double *wave,
+                          const double *gradient_wave, const double *hessian_wave, const double *H_prefactor1,
+                          const double *first_order_gradient_rho, const double *v_hartree_gradient,
+                          const double *first_order_rho, const double *v2rho2_batches,
+                          const double *v2rhosigma_batches, const double *v2sigma2_batches,
+                          const double *partition_tab, double *first_order_H) {
+  static const int ih[3][3] = {{0, 1, 2}, {1, 3, 4}, {2, 4, 5}};
   const long nb2 = (long)n_basis * n_basis;
+  const long nmb = n_max_batch_size, nbt = n_my_batches_work;
+  double *cs = NULL;
+  long cs_len = 0;
   for (int b = 0; b < n_my_batches_work; ++b) {
     const int nc = n_compute_c_batches[b];
     const int np = n_point_batches[b];
     if (nc <= 0) continue;
     const int ncp = ((nc + 3) / 4) * 4;
     const int *ib = i_basis_batches + (long)n_centers_basis_I * b;
-    const double *phi = wave + i_batch_2_wave_offset[b];
+    const long off = i_batch_2_wave_offset[b];
+    const double *phi = wave + off;
+    const double *gph = gradient_wave + 3 * off;
+    const double *hph = hessian_wave + 6 * off;
     const int *bmap = i_valid_point_2_i_full_points_map + n_point_batches_prefix_sum[b];
-    for (int t = 0; t < n_active; ++t) {
-      /* contract_sum_1 = 0.5 * w * v * phi (:145-177), then the symmetric
-       * rank-2k update (:192-205) and its scatter (:207-215). */
+    if ((long)nc * np > cs_len) {
+      free(cs);
+      cs_len = (long)nc * np;
+      cs = (double *)malloc(sizeof(double) * cs_len);
+    }
+    for (int ja = j_atom_begin; ja <= j_atom_end; ++ja) {
+      const int t = ja - j_atom_begin;
+      if (t >= T) break;
+      const int vs = atom_valid[(ja - 1) + (long)(n_atoms + 1) * b];
+      const int ve = atom_valid[ja + (long)(n_atoms + 1) * b];
+      for (int p = 0; p < np; ++p) {
+        const long f = bmap[p];
+        const long bp = p + nmb * (b + nbt * t);
+        const double pf1 = H_prefactor1[bp];
+        const double *fog = first_order_gradient_rho + 3 * bp;
+        const double *gr = gradient_rho + 3 * f;
+        const double vsig = vsigma_batches[3 * nmb * b + 3 * p];
+        const double v2r2 = v2rho2_batches[3 * nmb * b + 3 * p];
+        const double v2rs = v2rhosigma_batches[6 * nmb * b + 6 * p];
+        const double v2s2 = v2sigma2_batches[6 * nmb * b + 6 * p];
+        const double w = partition_tab[f];
+        const double r1 = first_order_rho[f + (long)n_full_points * t];
+        double lfos = 0.0;
+        for (int k = 0; k < 3; ++k) lfos += fog[k] * gr[k];
+        lfos *= 2.0;
+        double pf2[3], pf5[3];
+        for (int k = 0; k < 3; ++k) {
+          pf2[k] = 2.0 * w * gr[k] * (v2rs * r1 + v2s2 * lfos) + 2.0 * w * vsig * fog[k];
+          pf5[k] = 2.0 * vsig * w * gr[k];
+        }
+        const double pf3 = w * (v_hartree_gradient[f + (long)n_full_points * t] + v2r2 * r1 + v2rs * lfos);
+        for (int i = 0; i < nc; ++i) {
+          const double c1 = (pf1 + pf3) * phi[i + (long)ncp * p];
+          double c2 = 0.0;
+          for (int k = 0; k < 3; ++k) c2 += pf2[k] * gph[i + (long)ncp * (k + 3L * p)];
+          cs[i + (long)nc * p] = 0.5 * c1 + c2;
+        }
+        for (int i = vs; i < ve; ++i) {
+          double c5 = 0.0;
+          for (int k = 0; k < 3; ++k) c5 += pf5[k] * -hph[i + (long)ncp * (ih[k][j_coord - 1] + 6L * p)];
+          cs[i + (long)nc * p] += c5;
+        }
+      }
       for (int i = 0; i < nc; ++i)
-        for (int j = 0; j <= i; ++j) {
+        for (int j = i; j < nc; ++j) {
           double s = 0.0;
-          for (int p = 0; p < np; ++p) {
-            const int f = bmap[p];
-            const double wv = partition_tab[f] * v_hartree_gradient[f + (long)n_full_points * t];
-            const double c_i = 0.5 * (wv * phi[i + (long)ncp * p]);
-            const double c_j = 0.5 * (wv * phi[j + (long)ncp * p]);
-            s += c_i * phi[j + (long)ncp * p] + phi[i + (long)ncp * p] * c_j;
-          }
+          for (int p = 0; p < np; ++p)
+            s += cs[j + (long)nc * p] * phi[i + (long)ncp * p] + phi[j + (long)ncp * p] * cs[i + (long)nc * p];
           const long ai = ib[i] - 1, aj = ib[j] - 1;
+          double *Ht = first_order_H + nb2 * t;
           if (i == j) {
-            first_order_H[ai + n_basis * ai + nb2 * t] += s;
+            Ht[ai + n_basis * ai] += s;
           } else {
-            first_order_H[ai + n_basis * aj + nb2 * t] += s;
-            first_order_H[aj + n_basis * ai + nb2 * t] += s;
+            Ht[ai + n_basis * aj] += s;
+            Ht[aj + n_basis * ai] += s;
           }
         }
     }
   }
+  free(cs);
 }
 
 /* ------------------------------------------------------------------------ */

@@ -54,17 +54,22 @@ void oracle_sumup(int T, int j_atom_begin, int j_atom_end, int n_full_points, in
  * associated-Legendre recursion; l <= 8. Matches B/sheval.hpp:6-343. */
 void oracle_ylm(int l_max, double x, double y, double z, double *ylm);
 
-/* First-order H integration with every XC term zero
- * (B/evaluate_first_order_H.cpp:13-222 with vsigma = v2rho2 = v2rhosigma =
- * v2sigma2 = H_prefactor1 = 0): accumulates
- *   H(ib_i, ib_j, t) += sum_p w(p) v(p, t) phi_i(p) phi_j(p)
- * which equals dL/dP1 for L = sum_p w v rho1.  H is (n_basis, n_basis, T). */
+/* First-order H integration with every term (B/evaluate_first_order_H.cpp:13-222),
+ * argument order as the reference's (arrays in its layouts, atom_valid
+ * (n_atoms + 1, n_batches)); accumulates into first_order_H (n_basis, n_basis, T).
+ * With every XC array zero it is H(ib_i, ib_j, t) += sum_p w v phi_i phi_j,
+ * which equals dL/dP1 for L = sum_p w v rho1. */
 void oracle_first_order_h(int T, int n_my_batches_work, int j_atom_begin, int j_atom_end, int n_full_points,
-                          int n_basis, int n_centers_basis_I, const int *n_point_batches,
-                          const int *n_point_batches_prefix_sum, const int *i_valid_point_2_i_full_points_map,
-                          const int *n_compute_c_batches, const int *i_basis_batches,
-                          const int *i_batch_2_wave_offset, const double *wave, const double *partition_tab,
-                          const double *v_hartree_gradient, double *first_order_H);
+                          int j_coord, int n_basis, int n_max_batch_size, int n_centers_basis_I,
+                          const int *n_point_batches, const int *n_compute_c_batches, const int *i_basis_batches,
+                          const int *atom_valid, int n_atoms, const int *n_point_batches_prefix_sum,
+                          const int *i_valid_point_2_i_full_points_map, const double *vsigma_batches,
+                          const double *gradient_rho, const int *i_batch_2_wave_offset, const double *wave,
+                          const double *gradient_wave, const double *hessian_wave, const double *H_prefactor1,
+                          const double *first_order_gradient_rho, const double *v_hartree_gradient,
+                          const double *first_order_rho, const double *v2rho2_batches,
+                          const double *v2rhosigma_batches, const double *v2sigma2_batches,
+                          const double *partition_tab, double *first_order_H);
 
 /* Spherical-form far field, in long double, for validating multipole tables:
  * out[p] += sum_atoms sum_{l<=l_max, m} Q(l*l+l+m, atom) r^-(l+1) Y_lm(r_hat),

@@ -13,7 +13,9 @@ import os
 import re
 import sys
 
-ref = os.environ.get("FR_REF", "/root/reference")
+# the reference checkout: $FR_REF, else the directory `reference` beside this repository
+ref = os.environ.get("FR_REF") or os.path.join(
+    os.path.dirname(os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__))))), "reference")
 path = os.path.join(ref, "fast_rap_src_dfpt_gpu_eval", "sum_up_far_dist_potential_dot.hpp")
 src = open(path).read()
 body = src[src.index("sum_up_far_dist_potential_dot_spec"):]

@@ -92,6 +92,23 @@ def test_first_order_h_oracle_matches_reference():
     assert rel(oracle.first_order_h(p, v), oracle.first_order_h(p, v, use_reference=True)) < 1e-13
 
 
+@needs_reference(2)
+@pytest.mark.parametrize("j_coord", [1, 3])
+def test_first_order_h_oracle_with_every_term_matches_reference(j_coord):
+    p = synth.make_rho1_problem(T=2, seed=5, n_atoms=6, n_batches=16, pad_value=np.nan, n_active=2)
+    xc = synth.first_order_h_inputs(p, seed=11, pad_value=np.nan)
+    v = np.asfortranarray(np.random.default_rng(3).normal(size=(p.n_full_points, 2)))
+    ho = oracle.first_order_h(p, v, xc=xc, j_coord=j_coord)
+    hr = oracle.first_order_h(p, v, use_reference=True, xc=xc, j_coord=j_coord)
+    assert np.all(np.isfinite(ho)) and np.abs(ho).max() > 0
+    assert rel(ho, hr) < 1e-13
+    # every term moves the result (the test would not see a dropped term otherwise)
+    for k in xc:
+        xk = dict(xc)
+        xk[k] = np.zeros_like(xc[k])
+        assert rel(oracle.first_order_h(p, v, xc=xk, j_coord=j_coord), ho) > 1e-6, k
+
+
 @needs_reference(4)
 def test_bias_producer_oracle_matches_reference():
     p = synth.make_rho1_problem(T=4, seed=4, n_atoms=6, n_batches=20, pad_value=np.nan, n_active=3)

@@ -70,3 +70,62 @@ def test_noalloc_sumup_rejects_sizes_beyond_its_scratch():
     st = _noalloc(big, a, dv)
     assert st == _lib.FRPA_ERR_INVALID
     assert "scratch" in _lib.last_error()[1]
+
+
+def _noalloc_flags():
+    f = ctypes.c_int(-1)
+    assert _lib.lib().frpa_sumup_noalloc_flags(ctypes.byref(f), ctypes.c_void_p(0)) == 0, _lib.last_error()
+    return f.value
+
+
+def test_noalloc_sumup_partial_atom_tile_matches_plan():
+    # tile of 3 perturbations with only 2 active: columns t >= n_active stay untouched
+    p = synth.make_sumup_problem(n_atoms=16, n_points=3000, l_pot_max=5, T=3, n_active=2, seed=17,
+                                 extra_full_points=25)
+    assert p.j_atom_end - p.j_atom_begin + 1 == 2
+    a = _device_arrays(p)
+    plan = _lib.SumupPlan(p)
+    dv_plan, dv_noalloc = dev(p.delta_v_hartree), dev(p.delta_v_hartree)
+    d0 = p.delta_v_hartree.copy()
+    shape = (p.n_full_points, p.T)
+    plan.execute(2, a["lhmfd"], a["mrs"], a["opr"], a["Q"], a["spline"], dv_plan)
+    assert _noalloc(p, a, dv_noalloc) == 0, _lib.last_error()
+    torch.cuda.synchronize()
+    ref, got = host(dv_plan, shape), host(dv_noalloc, shape)
+    assert normwise_rel(got[:, :2] - d0[:, :2], ref[:, :2] - d0[:, :2]) < TOL
+    assert np.array_equal(got[:, 2], d0[:, 2])
+    plan.close()
+
+
+def test_noalloc_sumup_without_valid_points_leaves_output_unchanged():
+    p = synth.make_sumup_problem(n_atoms=6, n_points=200, l_pot_max=4, T=1, seed=5)
+    a = _device_arrays(p)
+    dv = dev(p.delta_v_hartree)
+    p.n_valid_points = 0
+    assert _noalloc(p, a, dv) == 0, _lib.last_error()
+    torch.cuda.synchronize()
+    assert np.array_equal(host(dv, (p.n_full_points, p.T)), p.delta_v_hartree)
+
+
+def test_noalloc_sumup_reports_clamped_far_distance_l():
+    # an l_hartree_max_far_distance entry above l_pot_max is clamped on the
+    # device; the flag word keeps it until frpa_sumup_noalloc_flags reads it
+    p = synth.make_sumup_problem(n_atoms=10, n_points=1500, l_pot_max=4, T=1, seed=23)
+    _noalloc_flags()  # start from a clear flag word
+    a = _device_arrays(p)
+    bad = p.l_hartree_max_far_distance.copy()
+    bad[3, 0] = p.l_pot_max + 2
+    a["lhmfd"] = dev(bad, np.int32)
+    plan = _lib.SumupPlan(p)
+    plan.device_flags()
+    dv_plan, dv_noalloc = dev(p.delta_v_hartree), dev(p.delta_v_hartree)
+    plan.execute(1, a["lhmfd"], a["mrs"], a["opr"], a["Q"], a["spline"], dv_plan)
+    assert _noalloc(p, a, dv_noalloc) == 0, _lib.last_error()
+    torch.cuda.synchronize()
+    assert plan.device_flags() & 1
+    assert _noalloc_flags() & 1
+    assert _noalloc_flags() == 0  # read and cleared
+    d0 = p.delta_v_hartree
+    shape = (p.n_full_points, p.T)
+    assert normwise_rel(host(dv_noalloc, shape) - d0, host(dv_plan, shape) - d0) < TOL
+    plan.close()
