@@ -55,6 +55,9 @@ def parse_args():
     ap.add_argument("--config4-sizes", default="2000",
                     help="config-4 sweep sizes in atoms (comma list; 2000,10000,40000 for the full sweep)")
     ap.add_argument("--no-config4", action="store_true", help="skip the config-4 sweep")
+    ap.add_argument("--no-config5", action="store_true", help="skip the adjoint / first-order H timings")
+    ap.add_argument("--scaling", choices=["weak", "strong"], default="weak",
+                    help="weak: each rank its own config-2 problem; strong: one problem, batches sharded by cost")
     ap.add_argument("--mode", choices=["fp64", "split", "i8"], default=None,
                     help="headline rho1 path (default: split if built, else fp64)")
     return ap.parse_args()
@@ -217,15 +220,21 @@ def _dev(a, dtype=None):
 
 
 class Rho1Workload:
-    """Config-2 batches with phi / grad phi generated on the device."""
+    """Config-2 batches with phi / grad phi generated on the device.  With
+    ``shard = (rank, world)`` the problem is the same on every rank and this
+    rank keeps its cost-balanced share of the batches (strong scaling)."""
 
-    def __init__(self, n_batches: int, seed: int):
+    def __init__(self, n_batches: int, seed: int, shard=None):
         import torch
 
-        from fast_rpa_eval_b200 import _lib, synth
+        from fast_rpa_eval_b200 import _lib, parallel, synth
 
         t0 = time.time()
         self.prob = p = synth.config2(seed=seed, n_batches=n_batches)
+        if shard is not None:
+            rank, world = shard
+            ids = parallel.shard_batches(parallel.rho1_batch_costs(p), world)[rank]
+            self.prob = p = parallel.select_batches(p, ids)
         self.t_host = time.time() - t0
         pts = _dev(np.asfortranarray(p.valid_points_xyz.T))
         self.wave = torch.empty(p.wave_len, dtype=torch.float64, device="cuda")
@@ -337,6 +346,71 @@ def time_sumup(L: int, n_points: int, seed: int, K: int, W: int, ranks: Ranks, s
     return p, ms, fast
 
 
+def time_config5(K: int, W: int, ranks: Ranks, stream, fp64_peak: float, fma_peak: float):
+    """Config 5 (the adjoint check): dL/dP1 and the first-order H with every
+    exchange-correlation term on the config-1 recipe at 200 atoms, and dL/dQ
+    of the sum-up at 100 atoms, l_max 6, 200,000 points.  Each call is timed
+    with CUDA events over K calls after W warm-up calls; FLOPs are the
+    contraction's 2 T nc^2 np (FP64 tensor pipe) and, for dQ, the forward's
+    2 (L + 1)^2 per evaluated (point, atom) pair (FP64 FMA pipe)."""
+    import torch
+
+    from fast_rpa_eval_b200 import _lib, synth
+
+    from fast_rpa_eval_b200 import parallel
+
+    out = {}
+    p = synth.make_rho1_problem(T=1, seed=5, n_atoms=200, box=None, density=0.1, n_batches=1600,
+                                nc_range=(40, 120), exact_selection=False)
+    if ranks.world > 1:  # each rank its cost share of the batches; dP1 summed over ranks (NCCL)
+        p = parallel.select_batches(p, parallel.shard_batches(parallel.rho1_batch_costs(p), ranks.world)[ranks.rank])
+    plan = _lib.Rho1Plan(p)
+    rng = np.random.default_rng(5)
+    w, gw = _dev(p.wave), _dev(p.gradient_wave)
+    g_rho = _dev(rng.uniform(0.01, 1.0, p.n_full_points) * rng.normal(size=p.n_full_points))
+    dP1 = torch.zeros(p.n_basis * p.n_basis, dtype=torch.float64, device="cuda")
+    gemm = 2.0 * float(np.sum(p.n_compute_c_batches.astype(np.float64) ** 2 * p.n_point_batches))
+    def adjoint_step():
+        plan.adjoint_p1(1, w, gw, g_rho, None, dP1, stream=stream)
+        if ranks.world > 1:
+            parallel.all_reduce_sum(dP1)
+
+    ms = time_device_steps(adjoint_step, K, W, ranks, stream)
+    gemm = ranks.sum(gemm)
+    out["adjoint_dP1"] = {"ms_per_call": ms, "tflops_fp64": gemm / (ms / 1e3) / 1e12,
+                          "frac_of_measured_fp64_mma": gemm / (ms / 1e3) / 1e12 / fp64_peak / ranks.world,
+                          "batches_per_rank": int(p.n_my_batches_work), "n_basis": int(p.n_basis),
+                          "accumulation": "128-bit fixed point, bit-identical across runs",
+                          "ranks": ranks.world,
+                          "collective": "NCCL all-reduce of dP1 after each call" if ranks.world > 1 else None}
+    xc = {k: _dev(a) for k, a in synth.first_order_h_inputs(p, seed=6).items()}
+    vhg, pt = _dev(rng.normal(size=p.n_full_points)), _dev(p.partition_tab)
+    av = torch.from_numpy(np.ascontiguousarray(p.atom_valid_n_compute_c_batches.ravel(order="F"),
+                                               dtype=np.int32)).cuda()
+    H = torch.zeros(p.n_basis * p.n_basis, dtype=torch.float64, device="cuda")
+    ms = time_device_steps(lambda: plan.first_order_h(1, p.n_atoms, 1, 1, av, w, gw, xc["hessian_wave"], xc, vhg,
+                                                      pt, H, stream=stream), K, W, ranks, stream)
+    out["first_order_h"] = {"ms_per_call": ms, "tflops_fp64": gemm / (ms / 1e3) / 1e12,
+                            "frac_of_measured_fp64_mma": gemm / (ms / 1e3) / 1e12 / fp64_peak / ranks.world,
+                            "terms": "H_prefactor1, v_hartree_gradient, vsigma/gradient terms, v2rho2, v2rhosigma, "
+                                     "v2sigma2, Hessian", "device_flags": plan.device_flags()}
+    del plan, w, gw, xc, H, dP1
+    s = synth.make_sumup_problem(n_atoms=100, n_points=200_000, l_pot_max=6, T=1, seed=9, outer_radius=8.0,
+                                 l_hartree_per_species=[6, 5, 4, 6])
+    sp = _lib.SumupPlan(s)
+    args = (_dev(s.l_hartree_max_far_distance, np.int32), _dev(s.multipole_radius_sq), _dev(s.outer_potential_radius),
+            _dev(s.multipole_moments))
+    g = _dev(rng.normal(size=s.n_full_points))
+    dQ = torch.empty(s.multipole_moments.size, dtype=torch.float64, device="cuda")
+    ms = time_device_steps(lambda: sp.adjoint_q(1, *args, g, dQ, stream=stream), K, W, ranks, stream)
+    flops = 2.0 * 49 * s.pair_count()
+    out["adjoint_dQ"] = {"ms_per_call": ms, "pairs": int(s.pair_count()),
+                         "tflops_convention_2L2": flops / (ms / 1e3) / 1e12,
+                         "frac_of_measured_fp64_fma": flops / (ms / 1e3) / 1e12 / fma_peak}
+    sp.close()
+    return out
+
+
 # ----------------------------------------------------------- CPU baseline
 
 
@@ -444,7 +518,10 @@ def run_frpa(args, ranks: Ranks):
     mode = {"split": _lib.RHO1_SPLIT_BF16, "i8": _lib.RHO1_SPLIT_I8}.get(mode_name, _lib.RHO1_FP64)
     out = {}
 
-    w = Rho1Workload(args.batches, seed=2 + 7919 * ranks.rank)
+    if args.scaling == "strong":  # one config-2 problem, its batches shared out by cost
+        w = Rho1Workload(args.batches, seed=2, shard=(ranks.rank, ranks.world))
+    else:  # every rank its own seeded config-2 problem
+        w = Rho1Workload(args.batches, seed=2 + 7919 * ranks.rank)
     p = w.prob
     info = w.plan.info()
     w_points, w_flops, w_bytes = int(p.total_points()), p.flops(), p.algorithmic_bytes()
@@ -505,7 +582,8 @@ def run_frpa(args, ranks: Ranks):
     i8_traffic = profile_traffic("rho1_split_i8_step", p.n_my_batches_work)
     out["rho1_split_i8"] = {
         "pts_per_s": total_pts / (ms_i8 / 1e3), "ms_per_step": ms_i8, "speedup_vs_fp64": ms_fp64 / ms_i8,
-        "kernels_per_group": "pack A (phi digits), pack B (P1c digits), tcgen05.mma.kind::i8 contraction",
+        "kernels_per_group": "pack A (phi digits), tcgen05.mma.kind::i8 contraction with P1c digits built in "
+                             "shared memory",
         "groups": i8_groups,
         "hbm_gbs_algorithmic": w_bytes / (ms_i8 / 1e3) / 1e9,
         "dram_bytes_per_step": i8_traffic,
@@ -529,6 +607,10 @@ def run_frpa(args, ranks: Ranks):
     out["bias_part2_4_atoms"] = {"ms_per_call": ms_bias, "pts_per_s": total_pts / (ms_bias / 1e3),
                                  "device_flags": w.plan.device_flags()}
     del av, bias4
+
+    # config 5: the adjoints and the first-order H (small; timed beside the headline)
+    if not args.no_config5:
+        out["config5"] = time_config5(args.steps, args.warmup, ranks, stream, fp64_peak, fma_peak)
 
     # end to end through the reference-named session entry point
     e2e = None
@@ -636,7 +718,8 @@ def run_frpa(args, ranks: Ranks):
                     "bf16_frac_of_measured": 15 * w_flops / (ms / 1e3) / 1e12 / peaks["bf16_tflops"]}
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": args.scaling,
+        "vs_baseline": None,
         "dtype": {_lib.RHO1_FP64: "f64",
                   _lib.RHO1_SPLIT_BF16: "f64 in/out, bf16x5 slices -> f32 (tcgen05) contraction",
                   _lib.RHO1_SPLIT_I8: "f64 in/out, int8x5 digit planes -> exact int32 level sums (tcgen05 kind::i8) "
@@ -647,16 +730,18 @@ def run_frpa(args, ranks: Ranks):
                    "path": mode_name, "valid_batches": info["n_valid_batches"], "work_items": n_items_tuned,
                    "launch": ("one persistent grouped launch per step, replayed from a CUDA graph"
                               if mode != _lib.RHO1_SPLIT_I8 else
-                              f"row max + {i8_groups} groups x (pack phi, pack P1c, contraction), "
+                              f"row max + {i8_groups} groups x (pack phi, contraction), "
                               "replayed from a CUDA graph"),
                    "tuning": tuned or "defaults (--no-tune)",
                    "grid_points_per_rank": w_points,
                    "l2": "inputs larger than L2 (phi + grad phi = %.1f GB per rank)" % (4 * 8 * p.wave_len / 1e9),
-                   "parallelism": f"weak, {args.gpus} independent shards"},
+                   "parallelism": (f"weak, {args.gpus} independent config-2 problems" if args.scaling == "weak" else
+                                   f"strong, one config-2 problem, batches sharded by cost over {args.gpus} ranks "
+                                   "(no collective on the forward path)")},
         "roofline": roofline,
         "clocks": clk,
         "gpu_launches": args.steps * {_lib.RHO1_FP64: 1, _lib.RHO1_SPLIT_BF16: 2,
-                                      _lib.RHO1_SPLIT_I8: 1 + 3 * i8_groups}[mode],
+                                      _lib.RHO1_SPLIT_I8: 1 + 2 * i8_groups}[mode],
         "cpu_baseline": cpu,
         "e2e": e2e,
         "measured_fp64_tflops": {"mma": fp64_peak, "fma": fma_peak},

@@ -207,11 +207,11 @@ class Rho1Plan:
         return {"n_items": out[0], "n_valid_batches": out[1], "n_valid_points": out[2]}
 
     def i8_info(self):
-        """Split-int8 grouping: groups (three launches each), work items,
-        packed P1c tiles, largest per-group A + B scratch in bytes."""
+        """Split-int8 grouping: groups (two launches each), point tiles,
+        contraction units, largest per-group packed-phi scratch in bytes."""
         out = (c_ll * 4)()
         check(lib().frpa_rho1_plan_i8_info(self.handle, out))
-        return {"groups": out[0], "items": out[1], "b_tiles": out[2], "scratch_bytes": out[3]}
+        return {"groups": out[0], "items": out[1], "units": out[2], "scratch_bytes": out[3]}
 
     def execute(self, n_active, wave, gwave, P1, bias, gbias, rho, grad, mode=RHO1_FP64, stream=None):
         check(lib().frpa_rho1_execute(self.handle, c_int(mode), c_int(n_active), _ptr(wave), _ptr(gwave), _ptr(P1),
@@ -245,6 +245,17 @@ class Rho1Plan:
             check(lib().frpa_rho1_plan_get_tuning(self.handle, c_int(key), ctypes.byref(v)))
             out[k] = v.value
         return out
+
+    def first_order_h(self, n_active, n_atoms, j_atom_begin, j_coord, atom_valid, wave, gwave, hwave, xc, vhg,
+                      partition_tab, H, stream=None):
+        """frpa_rho1_first_order_h: accumulates into H (device); ``xc`` maps
+        the names of synth.first_order_h_inputs to device tensors."""
+        check(lib().frpa_rho1_first_order_h(
+            self.handle, c_int(n_active), c_int(n_atoms), c_int(j_atom_begin), c_int(j_coord), _ptr(atom_valid),
+            _ptr(wave), _ptr(gwave), _ptr(hwave), _ptr(xc["vsigma"]), _ptr(xc["gradient_rho"]),
+            _ptr(xc["H_prefactor1"]), _ptr(xc["first_order_gradient_rho"]), _ptr(vhg), _ptr(xc["first_order_rho"]),
+            _ptr(xc["v2rho2"]), _ptr(xc["v2rhosigma"]), _ptr(xc["v2sigma2"]), _ptr(partition_tab), _ptr(H),
+            _stream(stream)))
 
     def adjoint_p1(self, n_active, wave, gwave, g_rho, g_grad, dP1, stream=None):
         check(lib().frpa_rho1_adjoint_p1(self.handle, c_int(n_active), _ptr(wave), _ptr(gwave), _ptr(g_rho),
@@ -358,6 +369,32 @@ def dropin_rho1(prob, symbol: str = "evaluate_first_order_rho_reduce_memory_c_v3
     check_void_call()
     return (np.asarray(rho).reshape((prob.n_full_points, T), order="F"),
             np.asarray(grad).reshape((3, prob.n_max_batch_size, prob.n_my_batches_work, T), order="F"))
+
+
+def dropin_first_order_h(prob, v_hartree_gradient, xc, H=None, j_coord: int | None = None):
+    """evaluate_first_order_h_reduce_memory_c_v2_ with host arrays: ``xc`` as
+    synth.first_order_h_inputs, H (n_basis, n_basis, T) accumulated into
+    (zeros if None); returns H."""
+    T = prob.T
+    set_atom_tile_size(T)
+    k = _Keep()
+    Hf = (np.zeros(prob.n_basis * prob.n_basis * T) if H is None
+          else np.array(H, dtype=np.float64).ravel(order="F").copy())
+    jc = prob.j_coord if j_coord is None else j_coord
+    z = np.zeros(1)
+    lib().frpa_clear_error()
+    lib().evaluate_first_order_h_reduce_memory_c_v2_(
+        _iref(prob.j_atom_begin), _iref(prob.j_atom_end), _iref(prob.n_full_points), _iref(jc), _iref(prob.n_basis),
+        _iref(prob.n_atoms), _iref(prob.n_max_compute_ham), _iref(prob.n_max_batch_size),
+        _iref(prob.n_my_batches_work), _iref(prob.n_centers_basis_I), k.i(prob.n_point_batches),
+        k.i(prob.n_compute_c_batches), k.i(prob.i_basis_batches), k.i(prob.atom_valid_n_compute_c_batches),
+        k.i(prob.n_point_batches_prefix_sum), k.i(prob.i_valid_point_2_i_full_points_map), k.d(z),
+        k.d(xc["vsigma"]), k.d(xc["gradient_rho"]), k.d(z), k.i(prob.i_batch_2_wave_offset), k.d(prob.wave),
+        k.d(prob.gradient_wave), k.d(xc["hessian_wave"]), _ptr(Hf), k.d(xc["H_prefactor1"]),
+        k.d(xc["first_order_gradient_rho"]), k.d(v_hartree_gradient), k.d(xc["first_order_rho"]), k.d(xc["v2rho2"]),
+        k.d(xc["v2rhosigma"]), k.d(xc["v2sigma2"]), k.d(prob.partition_tab), _iref(0))
+    check_void_call()
+    return Hf.reshape((prob.n_basis, prob.n_basis, T), order="F")
 
 
 def dropin_sumup(prob, delta_v=None):

@@ -4,7 +4,9 @@
 
 Each translation unit is compiled with nvcc (-gencode arch=compute_100a,code=sm_100a,
 static CUDA runtime) and linked into fast_rpa_eval_b200/lib/libfrpa.so.  Objects are
-rebuilt only when a source or header is newer.
+rebuilt only when a source or header is newer.  The sum-up's per-l_max Horner
+bodies (kelvin_horner.cuh) are generated into the build directory first by
+csrc/gen_kelvin.py.
 """
 from __future__ import annotations
 
@@ -23,7 +25,20 @@ LIB = os.path.join(LIBDIR, "libfrpa.so")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr",
-         "-I" + os.path.join(ROOT, "include"), "-I" + CSRC]
+         "-I" + os.path.join(ROOT, "include"), "-I" + CSRC, "-I" + BUILD]
+
+
+def generate_headers() -> list:
+    """Writes the generated headers into the build directory (unchanged
+    files are left alone, so their timestamps do not force rebuilds)."""
+    sys.path.insert(0, CSRC)
+    try:
+        import gen_kelvin
+    finally:
+        sys.path.pop(0)
+    dst = os.path.join(BUILD, "kelvin_horner.cuh")
+    gen_kelvin.write(dst)
+    return [dst]
 
 
 def _newer(target: str, deps) -> bool:
@@ -36,8 +51,9 @@ def _newer(target: str, deps) -> bool:
 def build(force: bool = False, verbose: bool = False) -> str:
     os.makedirs(BUILD, exist_ok=True)
     os.makedirs(LIBDIR, exist_ok=True)
+    generated = generate_headers()
     sources = sorted(glob.glob(os.path.join(CSRC, "*.cu")))
-    headers = glob.glob(os.path.join(CSRC, "*.cuh")) + [os.path.join(ROOT, "include", "frpa.h")]
+    headers = glob.glob(os.path.join(CSRC, "*.cuh")) + [os.path.join(ROOT, "include", "frpa.h")] + generated
     objs, jobs = [], []
     for src in sources:
         obj = os.path.join(BUILD, os.path.basename(src) + ".o")

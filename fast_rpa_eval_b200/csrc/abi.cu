@@ -66,6 +66,8 @@ static void rho1_plan_free(Rho1Plan *P) {
   cudaFree(P->d_map);
   cudaFree(P->d_counter);
   cudaFree(P->d_adj_items);
+  cudaFree(P->d_h1_items_sym);
+  cudaFree(P->d_h1_acc);
   cudaFree(P->d_items_split);
   cudaFree(P->d_rowmax);
   cudaFree(P->d_err);
@@ -181,10 +183,13 @@ static int rho1_plan_build(Rho1Plan **out, const frpa_rho1_desc *D) {
       preb[b] = D->n_point_batches_prefix_sum[b];
       offb[b] = D->i_batch_2_wave_offset[b];
     }
-    std::vector<unsigned char> adj;
-    rho1_adjoint_build_items(ncb.data(), npb.data(), ib_off.data(), preb.data(), offb.data(), nb, T, &adj);
-    P->n_adj_items = (int)(adj.size() / rho1_adjoint_item_size());
+    std::vector<unsigned char> adj, sym;
+    rho1_h1_build_items(ncb.data(), npb.data(), ib_off.data(), preb.data(), offb.data(), nb, T, false, &adj);
+    P->n_adj_items = (int)(adj.size() / rho1_h1_item_size());
     up(&P->d_adj_items, adj.data(), adj.size());
+    rho1_h1_build_items(ncb.data(), npb.data(), ib_off.data(), preb.data(), offb.data(), nb, T, true, &sym);
+    P->n_h1_items_sym = (int)(sym.size() / rho1_h1_item_size());
+    up(&P->d_h1_items_sym, sym.data(), sym.size());
   }
   if (st == FRPA_OK) {
     P->grid_fp64 = rho1_fp64_grid(P->device);
@@ -223,7 +228,7 @@ struct DevBuf {
   int dev = -1;
 };
 std::mutex g_buf_mu;
-DevBuf g_bufs[24];
+DevBuf g_bufs[48];
 
 int ensure(int slot, size_t bytes, void **out) {
   int dev = 0;
@@ -427,15 +432,15 @@ int frpa_rho1_plan_info(const frpa_rho1_plan *plan, long long *info3) {
 int frpa_rho1_plan_i8_info(const frpa_rho1_plan *plan, long long *info4) {
   if (!plan || !info4) return fail(FRPA_ERR_INVALID, "rho1: null argument");
   const Rho1Plan &P = *plan->p;
-  long long items = 0, tiles = 0, scratch = 0;
+  long long items = 0, units = 0, scratch = 0;
   for (const I8Group &g : P.i8_groups) {
     items += g.item1 - g.item0;
-    tiles += g.tile1 - g.tile0;
-    scratch = std::max(scratch, g.a_bytes + g.b_bytes);
+    units += g.unit1 - g.unit0;
+    scratch = std::max(scratch, g.a_bytes);
   }
   info4[0] = (long long)P.i8_groups.size();
   info4[1] = items;
-  info4[2] = tiles;
+  info4[2] = units;
   info4[3] = scratch;
   return FRPA_OK;
 }
@@ -526,12 +531,37 @@ int frpa_rho1_bias_part2(const frpa_rho1_plan *plan, int T, int n_atoms, int j_a
                                 gradient_wave, density_matrix, first_order_rho_bias_part2, (cudaStream_t)stream);
 }
 
+int frpa_rho1_first_order_h(const frpa_rho1_plan *plan, int n_active, int n_atoms, int j_atom_begin, int j_coord,
+                            const int *atom_valid, const double *wave, const double *gradient_wave,
+                            const double *hessian_wave, const double *vsigma, const double *gradient_rho,
+                            const double *H_prefactor1, const double *first_order_gradient_rho,
+                            const double *v_hartree_gradient, const double *first_order_rho, const double *v2rho2,
+                            const double *v2rhosigma, const double *v2sigma2, const double *partition_tab,
+                            double *first_order_H, void *stream) {
+  if (!plan) return fail(FRPA_ERR_INVALID, "first-order H: null plan");
+  Rho1Plan &P = *plan->p;
+  FRPA_CHECK_ARG(n_active >= 0 && n_active <= P.T, "first-order H: j_atom_end - j_atom_begin + 1 = %d outside 0..%d",
+                 n_active, P.T);
+  FRPA_CHECK_ARG(j_coord >= 1 && j_coord <= 3, "first-order H: j_coord %d outside 1..3", j_coord);
+  FRPA_CHECK_ARG(n_active == 0 || (j_atom_begin >= 1 && j_atom_begin + n_active - 1 <= n_atoms),
+                 "first-order H: atoms %d..%d outside 1..%d", j_atom_begin, j_atom_begin + n_active - 1, n_atoms);
+  FRPA_CHECK_ARG(first_order_H && atom_valid && vsigma && gradient_rho && H_prefactor1 && first_order_gradient_rho &&
+                     v_hartree_gradient && first_order_rho && v2rho2 && v2rhosigma && v2sigma2 && partition_tab,
+                 "first-order H: null device pointer");
+  FRPA_CHECK_ARG(P.n_items == 0 || (wave && gradient_wave && hessian_wave), "first-order H: null wave pointer");
+  if (n_active == 0) return FRPA_OK;
+  return rho1_first_order_h_run(P, n_active, n_atoms, j_atom_begin, j_coord, atom_valid, wave, gradient_wave,
+                                hessian_wave, vsigma, gradient_rho, H_prefactor1, first_order_gradient_rho,
+                                v_hartree_gradient, first_order_rho, v2rho2, v2rhosigma, v2sigma2, partition_tab,
+                                first_order_H, (cudaStream_t)stream);
+}
+
 int frpa_rho1_adjoint_p1(const frpa_rho1_plan *plan, int n_active, const double *wave, const double *gradient_wave,
                          const double *g_rho, const double *g_grad, double *dP1, void *stream) {
   if (!plan) return fail(FRPA_ERR_INVALID, "rho1: null plan");
   FRPA_CHECK_ARG(dP1 && (g_rho || g_grad), "rho1 adjoint: null output or no upstream gradient");
   FRPA_CHECK_ARG(n_active <= plan->p->T, "rho1 adjoint: n_active %d > tile %d", n_active, plan->p->T);
-  return rho1_adjoint_launch_items(*plan->p, plan->p->d_adj_items, plan->p->n_adj_items, n_active, wave,
+  return rho1_adjoint_run(*plan->p, n_active, wave,
                                    gradient_wave, g_rho, g_grad, dP1, (cudaStream_t)stream);
 }
 
@@ -638,6 +668,84 @@ void evaluate_first_order_rho_reduce_memory_c_v3_batches_atoms_(
   if (st == FRPA_OK) {
     cudaError_t e = cudaStreamSynchronize(s);
     if (e != cudaSuccess) fail(FRPA_ERR_CUDA, "rho1: %s", cudaGetErrorString(e));
+  }
+  rho1_plan_free(P);
+}
+
+void evaluate_first_order_h_reduce_memory_c_v2_(
+    int *j_atom_begin, int *j_atom_end, int *n_full_points, int *j_coord, int *n_basis, int *n_atoms,
+    int *n_max_compute_ham, int *n_max_batch_size, int *n_my_batches_work, int *n_centers_basis_I,
+    int *n_point_batches, int *n_compute_c_batches, int *i_basis_batches, int *atom_valid_n_compute_c_batches,
+    int *n_point_batches_prefix_sum, int *i_valid_point_2_i_full_points_map, double *vrho_batches,
+    double *vsigma_batches, double *gradient_rho, double *H_times_psi_batches_compress, int *i_batch_2_wave_offset,
+    double *wave_batches_compress, double *gradient_wave_batches_compress, double *hessian_wave_batches_compress,
+    double *first_order_H_tile, double *H_prefactor1_batches_tile, double *first_order_gradient_rho_batches_tile,
+    double *v_hartree_gradient, double *first_order_rho, double *v2rho2_batches, double *v2rhosigma_batches,
+    double *v2sigma2_batches, double *partition_tab, int *not_use) {
+  (void)n_max_compute_ham;
+  (void)vrho_batches;                  // unused by the reference as well
+  (void)H_times_psi_batches_compress;  // unused by the reference as well
+  (void)not_use;
+  std::lock_guard<std::mutex> lk(g_buf_mu);
+  clear_error();
+  const int T = g_tile;
+  if (!j_atom_begin || !j_atom_end || !n_my_batches_work || !n_atoms || !j_coord || !first_order_H_tile) {
+    fail(FRPA_ERR_INVALID, "first-order H: null argument");
+    return;
+  }
+  const int n_active = *j_atom_end - *j_atom_begin + 1;
+  if (n_active > T) {
+    fail(FRPA_ERR_INVALID, "first-order H: j_atom_end - j_atom_begin + 1 = %d > ATOM_TILE_SIZE %d", n_active, T);
+    return;
+  }
+  frpa_rho1_desc d = rho_desc_from_ref(T, n_my_batches_work, n_full_points, n_basis, n_centers_basis_I,
+                                       n_max_batch_size, n_point_batches, n_point_batches_prefix_sum,
+                                       i_valid_point_2_i_full_points_map, n_compute_c_batches, i_basis_batches,
+                                       i_batch_2_wave_offset);
+  Rho1Plan *P = nullptr;
+  if (rho1_plan_build(&P, &d) != FRPA_OK) return;
+  const int nb = d.n_my_batches_work, nmb = d.n_max_batch_size, nf = d.n_full_points;
+  const size_t wl = (size_t)P->wave_len, nH = (size_t)d.n_basis * d.n_basis * T;
+  const size_t nav = (size_t)(*n_atoms + 1) * nb, nbt = (size_t)nmb * nb;
+  double *w = nullptr, *gw = nullptr, *hw = nullptr, *vs = nullptr, *gr = nullptr, *pf1 = nullptr, *fog = nullptr,
+         *vhg = nullptr, *r1 = nullptr, *v2r2 = nullptr, *v2rs = nullptr, *v2s2 = nullptr, *pt = nullptr,
+         *H = nullptr;
+  int *av = nullptr;
+  cudaStream_t s = 0;
+  int st = FRPA_OK;
+  if (st == FRPA_OK) st = h2d(24, wave_batches_compress, wl, &w, s);
+  if (st == FRPA_OK) st = h2d(25, gradient_wave_batches_compress, 3 * wl, &gw, s);
+  if (st == FRPA_OK) st = h2d(26, hessian_wave_batches_compress, 6 * wl, &hw, s);
+  if (st == FRPA_OK) st = h2d(27, vsigma_batches, 3 * nbt, &vs, s);
+  if (st == FRPA_OK) st = h2d(28, gradient_rho, 3 * (size_t)nf, &gr, s);
+  if (st == FRPA_OK) st = h2d(29, H_prefactor1_batches_tile, nbt * T, &pf1, s);
+  if (st == FRPA_OK) st = h2d(30, first_order_gradient_rho_batches_tile, 3 * nbt * T, &fog, s);
+  if (st == FRPA_OK) st = h2d(31, v_hartree_gradient, (size_t)nf * T, &vhg, s);
+  if (st == FRPA_OK) st = h2d(32, first_order_rho, (size_t)nf * T, &r1, s);
+  if (st == FRPA_OK) st = h2d(33, v2rho2_batches, 3 * nbt, &v2r2, s);
+  if (st == FRPA_OK) st = h2d(34, v2rhosigma_batches, 6 * nbt, &v2rs, s);
+  if (st == FRPA_OK) st = h2d(35, v2sigma2_batches, 6 * nbt, &v2s2, s);
+  if (st == FRPA_OK) st = h2d(36, partition_tab, (size_t)nf, &pt, s);
+  if (st == FRPA_OK) st = h2d(37, first_order_H_tile, nH, &H, s);
+  if (st == FRPA_OK) st = h2d(38, atom_valid_n_compute_c_batches, nav, &av, s);
+  frpa_rho1_plan handle{P};
+  if (st == FRPA_OK)
+    st = frpa_rho1_first_order_h(&handle, std::max(0, n_active), *n_atoms, *j_atom_begin, *j_coord, av, w, gw, hw, vs,
+                                 gr, pf1, fog, vhg, r1, v2r2, v2rs, v2s2, pt, H, s);
+  if (st == FRPA_OK &&
+      cudaMemcpyAsync(first_order_H_tile, H, sizeof(double) * nH, cudaMemcpyDeviceToHost, s) != cudaSuccess)
+    st = fail(FRPA_ERR_CUDA, "first-order H: download failed");
+  if (st == FRPA_OK) {
+    cudaError_t e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) st = fail(FRPA_ERR_CUDA, "first-order H: %s", cudaGetErrorString(e));
+  }
+  if (st == FRPA_OK) {
+    int flags = 0;
+    if (cudaMemcpy(&flags, P->d_err, sizeof(int), cudaMemcpyDeviceToHost) == cudaSuccess && flags)
+      fail(FRPA_ERR_DEVICE_INPUT,
+           "first-order H: device input flags 0x%x (8: an atom's compute range leaves its batch, clipped; 16: a "
+           "non-finite input, result incomplete)",
+           flags);
   }
   rho1_plan_free(P);
 }

@@ -8,7 +8,10 @@ on the largest degree in use and one body per lam serves every l_pot_max.
 The code is emitted rather than left to template unrolling because nvcc's
 optimiser takes tens of minutes on the equivalent nested unrolled loops.
 
-    python gen_kelvin.py          (rewrites kelvin_horner.cuh next to it)
+The build (fast_rpa_eval_b200/build.py) writes it into its build directory
+before compiling; by hand:
+
+    python gen_kelvin.py <output path>
 """
 import os
 
@@ -57,7 +60,7 @@ def horner_body(lam, npts):
     return "\n".join(out)
 
 
-def main():
+def render() -> str:
     lines = [
         "// Generated by gen_kelvin.py: straight-line Horner evaluation of the",
         "// Kelvin-inverted far-field polynomial, degree-graded coefficient packing.",
@@ -112,10 +115,18 @@ def main():
     lines.append("")
     lines.append("}  // namespace frpa")
     lines.append("")
-    dst = os.path.join(os.path.dirname(os.path.abspath(__file__)), "kelvin_horner.cuh")
+    return "\n".join(lines)
+
+
+def write(dst: str) -> None:
+    text = render()
+    if os.path.exists(dst) and open(dst).read() == text:
+        return
     with open(dst, "w") as f:
-        f.write("\n".join(lines))
+        f.write(text)
 
 
 if __name__ == "__main__":
-    main()
+    import sys
+
+    write(sys.argv[1])

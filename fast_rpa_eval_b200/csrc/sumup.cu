@@ -96,6 +96,11 @@ struct SumupPlan {
   double *d_convT_f = nullptr;
   double *d_dcoef = nullptr;  // (n_coef, n_chp, T)
   double *d_dmc = nullptr;    // (mc_dim, n_atoms, T)
+  // deterministic adjoint: per point-block partial sums (n_coef, n_chp, T,
+  // adj_nz), reduced in block order; slots of each atom (CSR, ascending)
+  double *d_dcoef_part = nullptr;
+  int adj_nz = 1, adj_pts = 4096;
+  int *d_atom_slot_ptr = nullptr, *d_atom_slots = nullptr;
 };
 
 namespace {
@@ -447,9 +452,11 @@ int launch_fast(const SumupPlan &P, int n_active, const double *spline, double *
 
 constexpr int ADJ_KCH = 32;
 
-// dcoef[k, slot, t] += sum over this block's points of g(p, t) u^k / r for
-// far-field pairs with deg(k) <= lam (the derivative of the fast path's
-// Horner sum with respect to its coefficients).
+// part[k, slot, t, z] = sum over point block z's points of g(p, t) u^k / r
+// for far-field pairs with deg(k) <= lam (the derivative of the fast path's
+// Horner sum with respect to its coefficients); each block sums its points in
+// a fixed order, and sumup_dcoef_reduce_kernel adds the blocks in order, so
+// the result is the same on every run.
 __global__ void __launch_bounds__(SU_THREADS)
     sumup_dcoef_kernel(int n_valid, int n_full, const int *__restrict__ map, const double *__restrict__ coord,
                        int n_chp, int L, const double *__restrict__ recs, const double *__restrict__ g,
@@ -508,24 +515,38 @@ __global__ void __launch_bounds__(SU_THREADS)
     if (threadIdx.x < ADJ_KCH && k0 + threadIdx.x < NK) {
       double v = 0.0;
       for (int w = 0; w < SU_THREADS / 32; ++w) v += red[w][threadIdx.x];
-      atomicAdd(dcoef + (k0 + threadIdx.x) + (long long)NK * (slot + (long long)n_chp * t), v);
+      // this point block's partial, summed over the blocks in order later
+      dcoef[(k0 + threadIdx.x) + (long long)NK * (slot + (long long)n_chp * (t + (long long)gridDim.y * blockIdx.z))] = v;
     }
     __syncthreads();
   }
 }
 
-// dmc[n, atom(slot), t] += sum_k conv[k, n] dcoef[k, slot, t]
-__global__ void sumup_dmc_kernel(int n_chp, int n_atoms, int mc_dim, int n_coef, const int *__restrict__ chp,
-                                 const int *__restrict__ c2a, const int *__restrict__ convT_ptr,
+// dcoef[k, slot, t] = sum over the point blocks z, in order, of part[k, slot, t, z]
+__global__ void sumup_dcoef_reduce_kernel(long long n, int nz, const double *__restrict__ part,
+                                          double *__restrict__ dcoef) {
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n; e += (long long)gridDim.x * blockDim.x) {
+    double s = 0.0;
+    for (int z = 0; z < nz; ++z) s += part[e + n * z];
+    dcoef[e] = s;
+  }
+}
+
+// dmc[n, atom, t] = sum over the atom's slots, in ascending order, of
+// sum_k conv[k, n] dcoef[k, slot, t] (a gather: no two threads add into one
+// entry, so the result is the same on every run)
+__global__ void sumup_dmc_kernel(int n_chp, int n_atoms, int mc_dim, int n_coef, const int *__restrict__ slot_ptr,
+                                 const int *__restrict__ slots, const int *__restrict__ convT_ptr,
                                  const int *__restrict__ convT_k, const double *__restrict__ convT_f,
                                  const double *__restrict__ dcoef, double *__restrict__ dmc) {
-  const int slot = blockIdx.x, t = blockIdx.y;
-  const int atom = c2a[chp[slot] - 1] - 1;
-  const double *dc = dcoef + (long long)n_coef * (slot + (long long)n_chp * t);
+  const int atom = blockIdx.x, t = blockIdx.y;
   for (int n = threadIdx.x; n < mc_dim; n += blockDim.x) {
     double s = 0.0;
-    for (int e = convT_ptr[n]; e < convT_ptr[n + 1]; ++e) s += convT_f[e] * dc[convT_k[e]];
-    if (s != 0.0) atomicAdd(dmc + n + (long long)mc_dim * (atom + (long long)n_atoms * t), s);
+    for (int q = slot_ptr[atom]; q < slot_ptr[atom + 1]; ++q) {
+      const double *dc = dcoef + (long long)n_coef * (slots[q] + (long long)n_chp * t);
+      for (int e = convT_ptr[n]; e < convT_ptr[n + 1]; ++e) s += convT_f[e] * dc[convT_k[e]];
+    }
+    dmc[n + (long long)mc_dim * (atom + (long long)n_atoms * t)] = s;
   }
 }
 
@@ -553,10 +574,13 @@ __global__ void sumup_dq_kernel(int n_atoms, int L, int L2, int mc_dim, int icc_
 }
 
 int launch_dcoef(const SumupPlan &P, int n_active, const double *g, cudaStream_t stream) {
-  const int pts = 4096;
-  const dim3 grid(P.n_chp, n_active, (P.n_valid_points + pts - 1) / pts);
+  const dim3 grid(P.n_chp, n_active, P.adj_nz);
   sumup_dcoef_kernel<<<grid, SU_THREADS, 0, stream>>>(P.n_valid_points, P.n_full_points, P.d_map, P.d_coord,
-                                                       P.n_chp, P.L, P.d_recs, g, pts, P.d_dcoef);
+                                                       P.n_chp, P.L, P.d_recs, g, P.adj_pts, P.d_dcoef_part);
+  FRPA_LAUNCH_CHECK();
+  const long long n = (long long)P.n_coef * P.n_chp * n_active;
+  sumup_dcoef_reduce_kernel<<<(int)std::min<long long>(4096, (n + 255) / 256), 256, 0, stream>>>(
+      n, P.adj_nz, P.d_dcoef_part, P.d_dcoef);
   FRPA_LAUNCH_CHECK();
   return FRPA_OK;
 }
@@ -623,7 +647,8 @@ void sumup_plan_free(SumupPlan *P) {
   void *ptrs[] = {P->d_map, P->d_order, P->d_coord, P->d_species, P->d_species_center, P->d_l_hartree, P->d_n_grid,
                   P->d_c2a, P->d_chp, P->d_icc, P->d_ncc, P->d_ijkmax, P->d_icc_packed, P->d_cc, P->d_cc_xyz,
                   P->d_rgm, P->d_linc, P->d_conv_ptr, P->d_conv_n, P->d_conv_f, P->d_mc, P->d_recs, P->d_err,
-                  P->d_convT_ptr, P->d_convT_k, P->d_convT_f, P->d_dcoef, P->d_dmc};
+                  P->d_convT_ptr, P->d_convT_k, P->d_convT_f, P->d_dcoef, P->d_dmc, P->d_dcoef_part,
+                  P->d_atom_slot_ptr, P->d_atom_slots};
   for (void *p : ptrs)
     if (p) cudaFree(p);
   delete P;
@@ -834,6 +859,30 @@ int sumup_plan_create(SumupPlan **out, const frpa_sumup_desc *D) {
   if (st == FRPA_OK &&
       cudaMalloc((void **)&P->d_dmc, sizeof(double) * (size_t)P->mc_dim * P->n_atoms * T) != cudaSuccess)
     st = fail(FRPA_ERR_OOM, "sumup: workspace allocation failed");
+  // adjoint: at most 64 point blocks per (slot, t), partials reduced in order
+  P->adj_pts = std::max(4096, (P->n_valid_points + 63) / 64);
+  P->adj_nz = std::max(1, (P->n_valid_points + P->adj_pts - 1) / P->adj_pts);
+  if (st == FRPA_OK && cudaMalloc((void **)&P->d_dcoef_part, sizeof(double) * (size_t)n_kelvin(L) *
+                                                                 std::max(1, P->n_chp) * T * P->adj_nz) != cudaSuccess)
+    st = fail(FRPA_ERR_OOM, "sumup: workspace allocation failed");
+  {
+    std::vector<int> cnt(P->n_atoms + 1, 0), slots(std::max(1, P->n_chp));
+    std::vector<int> atom_of(std::max(1, P->n_chp));
+    for (int q = 0; q < P->n_chp; ++q) {
+      atom_of[q] = D->center_to_atom[D->centers_hartree_potential[q] - 1] - 1;
+      ++cnt[atom_of[q] + 1];
+    }
+    for (int a = 0; a < P->n_atoms; ++a) cnt[a + 1] += cnt[a];
+    std::vector<int> fill(cnt.begin(), cnt.end() - 1);
+    for (int q = 0; q < P->n_chp; ++q) slots[fill[atom_of[q]]++] = q;  // ascending within each atom
+    if (st == FRPA_OK && (cudaMalloc((void **)&P->d_atom_slot_ptr, sizeof(int) * cnt.size()) != cudaSuccess ||
+                          cudaMalloc((void **)&P->d_atom_slots, sizeof(int) * slots.size()) != cudaSuccess))
+      st = fail(FRPA_ERR_OOM, "sumup: workspace allocation failed");
+    if (st == FRPA_OK &&
+        (cudaMemcpy(P->d_atom_slot_ptr, cnt.data(), sizeof(int) * cnt.size(), cudaMemcpyHostToDevice) != cudaSuccess ||
+         cudaMemcpy(P->d_atom_slots, slots.data(), sizeof(int) * slots.size(), cudaMemcpyHostToDevice) != cudaSuccess))
+      st = fail(FRPA_ERR_CUDA, "sumup: upload failed");
+  }
   if (st == FRPA_OK && cudaMalloc((void **)&P->d_mc, sizeof(double) * (size_t)P->mc_dim * P->n_atoms * T) != cudaSuccess)
     st = fail(FRPA_ERR_OOM, "sumup: workspace allocation failed");
   if (st == FRPA_OK &&
@@ -888,13 +937,13 @@ int sumup_read_error_flags(const SumupPlan *P, int *flags) {
 
 int sumup_adjoint_q(const SumupPlan *P, int n_active, const int *lhmfd, const double *mrs, const double *opr,
                     const double *Q, const double *g, double *dQ, cudaStream_t stream) {
-  FRPA_CHECK_ARG(P->fast, "sumup adjoint: needs the fast path (identity centers_hartree_potential and a "
-                          "homogeneous multipole table)");
+  if (!P->fast)
+    return fail(FRPA_ERR_UNSUPPORTED,
+                "sumup adjoint: dQ is implemented for the fast path only (identity centers_hartree_potential and a "
+                "homogeneous multipole table); this plan uses the generic far-field kernel");
   FRPA_CHECK_ARG(n_active >= 0 && n_active <= P->T, "sumup adjoint: n_active %d", n_active);
   FRPA_CUDA_TRY(cudaMemsetAsync(dQ, 0, sizeof(double) * (size_t)P->L2 * P->n_atoms * P->T, stream));
   if (n_active == 0 || P->n_chp == 0 || P->n_valid_points == 0) return FRPA_OK;
-  FRPA_CUDA_TRY(cudaMemsetAsync(P->d_dcoef, 0, sizeof(double) * (size_t)P->n_coef * P->n_chp * P->T, stream));
-  FRPA_CUDA_TRY(cudaMemsetAsync(P->d_dmc, 0, sizeof(double) * (size_t)P->mc_dim * P->n_atoms * P->T, stream));
   sumup_multipole_c_kernel<<<dim3(P->n_atoms, n_active), 128, 0, stream>>>(
       P->n_atoms, P->L, P->L2, P->mc_dim, P->icc_dim0, P->lma, P->d_icc, P->d_ncc, P->d_cc, lhmfd, Q, P->d_mc,
       P->d_err);
@@ -907,9 +956,9 @@ int sumup_adjoint_q(const SumupPlan *P, int n_active, const int *lhmfd, const do
   int st = FRPA_OK;
   st = launch_dcoef(*P, n_active, g, stream);
   if (st != FRPA_OK) return st;
-  sumup_dmc_kernel<<<dim3(P->n_chp, n_active), 128, 0, stream>>>(P->n_chp, P->n_atoms, P->mc_dim, P->n_coef,
-                                                                  P->d_chp, P->d_c2a, P->d_convT_ptr, P->d_convT_k,
-                                                                  P->d_convT_f, P->d_dcoef, P->d_dmc);
+  sumup_dmc_kernel<<<dim3(P->n_atoms, n_active), 128, 0, stream>>>(
+      P->n_chp, P->n_atoms, P->mc_dim, P->n_coef, P->d_atom_slot_ptr, P->d_atom_slots, P->d_convT_ptr, P->d_convT_k,
+      P->d_convT_f, P->d_dcoef, P->d_dmc);
   FRPA_LAUNCH_CHECK();
   sumup_dq_kernel<<<dim3(P->n_atoms, n_active), 64, 0, stream>>>(P->n_atoms, P->L, P->L2, P->mc_dim, P->icc_dim0,
                                                                   P->d_icc, P->d_ncc, P->d_cc, lhmfd, Q, P->d_dmc, dQ);

@@ -63,7 +63,10 @@ def select_batches(prob, batch_ids) -> object:
     new_off[1:] = np.cumsum(blk)
     pmap = np.concatenate([prob.i_valid_point_2_i_full_points_map[pre[b]:pre[b + 1]] for b in ids]) if len(ids) \
         else np.zeros(0, dtype=np.int32)
-    wave = gwave = None
+    wave = gwave = xyz = None
+    if prob.valid_points_xyz is not None:  # the points' coordinates, for a device phi generator
+        xyz = np.concatenate([prob.valid_points_xyz[pre[b]:pre[b + 1]] for b in ids]) if len(ids) \
+            else np.zeros((0, 3))
     if prob.wave is not None:
         wave = np.concatenate([prob.wave[off[b]:off[b + 1]] for b in ids]) if len(ids) else np.zeros(0)
         gwave = np.concatenate([prob.gradient_wave[3 * off[b]:3 * off[b + 1]] for b in ids]) if len(ids) \
@@ -77,7 +80,7 @@ def select_batches(prob, batch_ids) -> object:
         i_batch_2_wave_offset=new_off.astype(np.int32), wave=wave, gradient_wave=gwave,
         first_order_rho_bias_part2=np.asfortranarray(prob.first_order_rho_bias_part2[:, ids, :]),
         first_order_gradient_rho_bias=np.asfortranarray(prob.first_order_gradient_rho_bias[:, :, ids, :]),
-        valid_points_xyz=None)
+        valid_points_xyz=xyz)
 
 
 def merge_rho1(prob, parts):

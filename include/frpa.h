@@ -62,7 +62,8 @@ int frpa_get_atom_tile_size(void);
  *   FRPA_RHO1_FP64        FP64 tensor-core tiles (DMMA), the reference's arithmetic;
  *   FRPA_RHO1_SPLIT_BF16  five BF16 slices per operand on tcgen05 kind::f16, FP32 level sums;
  *   FRPA_RHO1_SPLIT_I8    five signed 8-bit digits per operand on tcgen05 kind::i8, exact
- *                         int32 level sums, operands packed by separate kernels. */
+ *                         int32 level sums; phi packed by a separate kernel, P1c built
+ *                         in shared memory by the contraction. */
 enum { FRPA_RHO1_FP64 = 0, FRPA_RHO1_SPLIT_BF16 = 1, FRPA_RHO1_SPLIT_I8 = 2 };
 int frpa_set_rho1_mode(int mode);
 int frpa_get_rho1_mode(void);
@@ -179,6 +180,29 @@ void generate_first_order_rho_bias_part2_(
     int *i_batch_2_wave_offset, double *wave_batches_compress, double *gradient_wave_batches_compress,
     double *first_order_rho_bias_part2, double *partition_tab, double *density_matrix);
 
+/* Replaces evaluate_first_order_h_reduce_memory_c_v2_
+ * (evaluate_first_order_H.h:3-43, CPU implementation evaluate_first_order_H.cpp:13-222):
+ * the first-order H integration with every term -- H_prefactor1,
+ * v_hartree_gradient, vsigma / gradient_rho / first_order_gradient_rho,
+ * v2rho2, v2rhosigma, v2sigma2 (their first components, as the reference reads
+ * them) and the Hessian term over each atom's compute functions -- for atoms
+ * j_atom_begin..j_atom_end (at most ATOM_TILE_SIZE), ACCUMULATED into
+ * first_order_H_tile (n_basis, n_basis, ATOM_TILE_SIZE) as in the reference.
+ * Host arrays, same layouts; vrho_batches, H_times_psi_batches_compress,
+ * n_max_compute_ham and not_use are accepted and unused, as in the reference.
+ * The result does not depend on the order in which batches meet in the
+ * output (bit-identical from run to run). */
+void evaluate_first_order_h_reduce_memory_c_v2_(
+    int *j_atom_begin, int *j_atom_end, int *n_full_points, int *j_coord, int *n_basis, int *n_atoms,
+    int *n_max_compute_ham, int *n_max_batch_size, int *n_my_batches_work, int *n_centers_basis_I,
+    int *n_point_batches, int *n_compute_c_batches, int *i_basis_batches, int *atom_valid_n_compute_c_batches,
+    int *n_point_batches_prefix_sum, int *i_valid_point_2_i_full_points_map, double *vrho_batches,
+    double *vsigma_batches, double *gradient_rho, double *H_times_psi_batches_compress, int *i_batch_2_wave_offset,
+    double *wave_batches_compress, double *gradient_wave_batches_compress, double *hessian_wave_batches_compress,
+    double *first_order_H_tile, double *H_prefactor1_batches_tile, double *first_order_gradient_rho_batches_tile,
+    double *v_hartree_gradient, double *first_order_rho, double *v2rho2_batches, double *v2rhosigma_batches,
+    double *v2sigma2_batches, double *partition_tab, int *not_use);
+
 /* The reference's device session.  The reference declares these four with
  * C++ linkage (device.hpp:191-192, device_data.hpp:159-227); as for the sum-up
  * cu_host_ entry point above, C++ code including this header binds the
@@ -253,9 +277,9 @@ int frpa_rho1_plan_create(frpa_rho1_plan **plan, const frpa_rho1_desc *desc);
 int frpa_rho1_plan_destroy(frpa_rho1_plan *plan);
 /* Work-list statistics: [n_items, n_valid_batches, n_valid_points]. */
 int frpa_rho1_plan_info(const frpa_rho1_plan *plan, long long *info3);
-/* Split-int8 mode: [groups, work items, packed P1c tiles, largest A + B scratch
- * of a group in bytes] (no counterpart in the reference).  Each group is three
- * kernel launches (pack phi, pack P1c, contraction). */
+/* Split-int8 mode: [groups, point tiles, contraction units, largest packed-phi
+ * scratch of a group in bytes] (no counterpart in the reference).  Each group
+ * is two kernel launches (pack phi, contraction with P1c built on chip). */
 int frpa_rho1_plan_i8_info(const frpa_rho1_plan *plan, long long *info4);
 
 /* rho1 and grad rho1 for perturbations t < T; rho1 is written for
@@ -303,14 +327,42 @@ enum {
 int frpa_rho1_plan_set_tuning(frpa_rho1_plan *plan, int key, int value);
 int frpa_rho1_plan_get_tuning(const frpa_rho1_plan *plan, int key, int *value);
 
+/* The first-order H on the device with a plan's work list (the drop-in
+ * evaluate_first_order_h_reduce_memory_c_v2_ runs this): perturbation t is
+ * atom j_atom_begin + t (1-based), t < n_active <= T.  Device arrays in the
+ * reference layouts: atom_valid (n_atoms + 1, n_batches), hessian_wave
+ * (6 x the wave length), vsigma (3, nmb, nb), gradient_rho (3, n_full),
+ * H_prefactor1 (nmb, nb, T), first_order_gradient_rho (3, nmb, nb, T),
+ * v_hartree_gradient and first_order_rho (n_full, T), v2rho2 (3, nmb, nb),
+ * v2rhosigma and v2sigma2 (6, nmb, nb), partition_tab (n_full).
+ * first_order_H (n_basis, n_basis, T) is accumulated into.  The per-batch
+ * contributions are added as 128-bit fixed-point integers, so the result is
+ * the same bits on every run whatever the order of the additions.  The
+ * accumulator ((n_basis, n_basis, T) x 16 bytes, shared with the adjoint) is
+ * allocated by the plan's first such call: make it before any stream capture.
+ * Device flags (frpa_rho1_device_flags): bit 3 an atom's compute range
+ * leaves its batch (clipped), bit 4 a non-finite input (result incomplete). */
+int frpa_rho1_first_order_h(const frpa_rho1_plan *plan, int n_active, int n_atoms, int j_atom_begin, int j_coord,
+                            const int *atom_valid, const double *wave, const double *gradient_wave,
+                            const double *hessian_wave, const double *vsigma, const double *gradient_rho,
+                            const double *H_prefactor1, const double *first_order_gradient_rho,
+                            const double *v_hartree_gradient, const double *first_order_rho, const double *v2rho2,
+                            const double *v2rhosigma, const double *v2sigma2, const double *partition_tab,
+                            double *first_order_H, void *stream);
+
 /* Adjoint: dP1 (n_basis, n_basis, T) += d(sum g_rho . rho1 + sum g_grad . grad)/dP1.
- * g_rho (n_full_points, T) or NULL, g_grad like grad or NULL.  dP1 is NOT zeroed. */
+ * g_rho (n_full_points, T) or NULL, g_grad like grad or NULL.  dP1 is NOT zeroed.
+ * Same engine and accumulation as frpa_rho1_first_order_h: deterministic
+ * (bit-identical from run to run); the first call allocates the accumulator. */
 int frpa_rho1_adjoint_p1(const frpa_rho1_plan *plan, int n_active, const double *wave, const double *gradient_wave,
                          const double *g_rho, const double *g_grad, double *dP1, void *stream);
 
-/* Reads and clears the device-side status of the plan's split-BF16 kernel:
- * bit 1 = a pipeline wait timed out (the kernel gave up and left its outputs
- * incomplete), bit 2 = its final drain timed out.  0 after a good run. */
+/* Reads and clears the device-side status of the plan's kernels: bit 1 = a
+ * pipeline wait of a tensor-core kernel timed out (the kernel gave up and left
+ * its outputs incomplete), bit 2 = its final drain timed out, bit 3 = an
+ * atom's compute range (atom_valid) left its batch and was clipped (bias and
+ * first-order H), bit 4 = a non-finite input reached the first-order H or
+ * adjoint accumulation.  0 after a good run. */
 int frpa_rho1_device_flags(const frpa_rho1_plan *plan, int *flags);
 
 typedef struct frpa_sumup_plan frpa_sumup_plan;
@@ -348,7 +400,9 @@ int frpa_sumup_execute(const frpa_sumup_plan *plan, int n_active, int flags, con
 
 /* Adjoint of the sum-up with respect to the multipole moments:
  * dQ ((l_pot_max+1)^2, n_atoms, T) = d(sum_p g(p, t) delta_v(p, t))/dQ, zeroed
- * first.  Needs the fast path (frpa_sumup_plan_fast). */
+ * first.  Implemented for the fast path (frpa_sumup_plan_fast); a plan on the
+ * generic kernel returns FRPA_ERR_UNSUPPORTED.  Partial sums are reduced in a
+ * fixed order: the same bits on every run. */
 int frpa_sumup_adjoint_q(const frpa_sumup_plan *plan, int n_active, const int *l_hartree_max_far_distance,
                          const double *multipole_radius_sq, const double *outer_potential_radius,
                          const double *multipole_moments, const double *g, double *dQ, void *stream);

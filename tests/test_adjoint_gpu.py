@@ -106,3 +106,33 @@ def test_dQ_central_finite_differences_config5_recipe():
     errs = [abs(_loss_fd(loss, Q.detach(), int(i), 1e-6) - float(g[int(i)])) for i in idx]
     scale = max(1.0, float(np.max(np.abs(g.cpu().numpy()[idx]))))
     assert max(errs) / scale < 1e-7, (max(errs), scale)
+
+
+def test_dQ_is_bit_identical_across_runs():
+    p = synth.make_sumup_problem(n_atoms=40, n_points=60_000, l_pot_max=6, T=2, seed=19, outer_radius=8.0)
+    plan = _lib.SumupPlan(p)
+    rng = np.random.default_rng(19)
+    args = (dev(p.l_hartree_max_far_distance, np.int32), dev(p.multipole_radius_sq), dev(p.outer_potential_radius),
+            dev(p.multipole_moments))
+    g = dev(rng.normal(size=(p.n_full_points, 2)))
+    outs = []
+    for _ in range(3):
+        dQ = torch.empty(p.multipole_moments.size, dtype=torch.float64, device="cuda")
+        plan.adjoint_q(2, *args, g, dQ)
+        torch.cuda.synchronize()
+        outs.append(dQ.clone())
+    assert torch.equal(outs[0], outs[1]) and torch.equal(outs[0], outs[2])
+    assert float(outs[0].abs().max()) > 0
+
+
+def test_dQ_on_the_generic_path_is_reported_unsupported():
+    # centres that are not the identity list put the plan on the generic kernel
+    p = synth.make_sumup_problem(n_atoms=12, n_points=2000, l_pot_max=4, T=1, seed=21, centers="permuted")
+    plan = _lib.SumupPlan(p)
+    assert not plan.fast
+    args = (dev(p.l_hartree_max_far_distance, np.int32), dev(p.multipole_radius_sq), dev(p.outer_potential_radius),
+            dev(p.multipole_moments))
+    dQ = torch.empty(p.multipole_moments.size, dtype=torch.float64, device="cuda")
+    with pytest.raises(_lib.FrpaError) as e:
+        plan.adjoint_q(1, *args, dev(p.delta_v_hartree), dQ)
+    assert e.value.status == _lib.FRPA_ERR_UNSUPPORTED and "fast path" in e.value.message

@@ -5,9 +5,12 @@ the sum-up points, evaluate their shards with the oracle, and reassemble.
   (batches are independent);
 * dL/dP1 (first-order H) summed over ranks by the all-reduce equals the
   unsharded integral to rounding;
-* the sum-up from point shards equals the unsharded result bit for bit.
+* the sum-up from point shards equals the unsharded result bit for bit;
+* dL/dQ_lm of the sum-up from point shards, summed by the all-reduce, equals
+  the unsharded one to rounding.
 """
 
+import dataclasses
 import datetime
 import os
 import socket
@@ -34,6 +37,25 @@ def _problems():
     return prob, sp
 
 
+def _dq_by_linearity(sp, g):
+    """dQ_lm(a) = sum_p g(p) d delta_v(p)/dQ_lm(a) for the moments the forward
+    keeps (|Q| > 1e-10): the sum-up is linear in them, so each column is one
+    oracle call with a unit moment and the near field (spline) off."""
+    L2 = (sp.l_pot_max + 1) ** 2
+    zero_spline = np.zeros_like(sp.spline)
+    zero_dv = np.zeros_like(sp.delta_v_hartree)
+    dQ = np.zeros((L2, sp.n_atoms))
+    for a in range(sp.n_atoms):
+        for lm in range(L2):
+            if abs(sp.multipole_moments[lm, a, 0]) <= 1e-10:
+                continue
+            Q = np.zeros_like(sp.multipole_moments)
+            Q[lm, a, 0] = 1.0
+            one = dataclasses.replace(sp, multipole_moments=Q, spline=zero_spline, delta_v_hartree=zero_dv)
+            dQ[lm, a] = float(np.dot(g, oracle.sumup(one)[:, 0]))
+    return dQ
+
+
 def _worker(rank: int, world: int, port: int, out_dir: str):
     os.environ["MASTER_ADDR"] = "127.0.0.1"
     os.environ["MASTER_PORT"] = str(port)
@@ -54,13 +76,17 @@ def _worker(rank: int, world: int, port: int, out_dir: str):
         dv = oracle.sumup(parallel.select_points(sp, sl))
         dparts = [None] * world
         dist.all_gather_object(dparts, (sl, dv))
+        # sum-up adjoint: this rank's points' share of dL/dQ, summed over ranks
+        gq = np.random.default_rng(7).standard_normal(sp.n_full_points)
+        dQ = torch.from_numpy(_dq_by_linearity(parallel.select_points(sp, sl), gq))
+        parallel.all_reduce_sum(dQ)
         if rank == 0:
             rho, grad = parallel.merge_rho1(prob, parts)
             dv_all = np.array(sp.delta_v_hartree, dtype=np.float64).reshape((sp.n_full_points, sp.T), order="F").copy()
             for s, d in dparts:
                 pts = sp.i_valid_point_2_i_full_points_map[s]
                 dv_all[pts, :] = d[pts, :]
-            np.savez(os.path.join(out_dir, "merged.npz"), rho=rho, grad=grad, H=H.numpy(), dv=dv_all)
+            np.savez(os.path.join(out_dir, "merged.npz"), rho=rho, grad=grad, H=H.numpy(), dv=dv_all, dQ=dQ.numpy())
         dist.barrier()
     finally:
         dist.destroy_process_group()
@@ -105,6 +131,9 @@ def test_two_gloo_ranks_reassemble_the_unsharded_results(tmp_path):
     H0 = oracle.first_order_h(prob, v)
     assert np.max(np.abs(got["H"] - H0)) <= 1e-13 * np.max(np.abs(H0))
     assert np.array_equal(got["dv"], oracle.sumup(sp))
+    dQ0 = _dq_by_linearity(sp, np.random.default_rng(7).standard_normal(sp.n_full_points))
+    assert np.abs(dQ0).max() > 0
+    assert np.max(np.abs(got["dQ"] - dQ0)) <= 1e-12 * np.max(np.abs(dQ0))
 
 
 @pytest.mark.gpu
