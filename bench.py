@@ -604,6 +604,26 @@ def run_frpa(args, ranks: Ranks):
         w.plan.bias_part2(4, p.n_atoms, 1, na, 1, av, w.wave, w.gwave, w.P1, bias4)
 
     ms_bias = time_device_steps(bias_step, args.steps, args.warmup, ranks, stream)
+
+    # rho1 with the density-matrix bias of atom 1 computed in the same launch,
+    # against the two-launch form (bias producer, then plain FP64 rho1)
+    bias1 = torch.zeros(p.n_max_batch_size * p.n_my_batches_work, dtype=torch.float64, device="cuda")
+
+    def fused_step():
+        w.plan.execute_fused_bias(1, p.n_atoms, 1, 1, av, w.P1, w.wave, w.gwave, w.P1, w.bias, w.gbias, w.rho, w.grad,
+                                  stream=stream)
+
+    def two_launch_step():
+        w.plan.bias_part2(1, p.n_atoms, 1, 1, 1, av, w.wave, w.gwave, w.P1, bias1, stream=stream)
+        w.step(_lib.RHO1_FP64, stream)
+
+    ms_fused = time_device_steps(fused_step, args.steps, args.warmup, ranks, stream)
+    ms_two = time_device_steps(two_launch_step, args.steps, args.warmup, ranks, stream)
+    out["rho1_fused_bias_1_atom"] = {"ms_fused": ms_fused, "ms_two_launches": ms_two,
+                                     "device_flags": w.plan.device_flags(),
+                                     "note": "fused: FP64 rho1 + density-matrix bias in one launch; two launches: "
+                                             "bias producer then FP64 rho1 (P1 stands in for the density matrix)"}
+    del bias1
     out["bias_part2_4_atoms"] = {"ms_per_call": ms_bias, "pts_per_s": total_pts / (ms_bias / 1e3),
                                  "device_flags": w.plan.device_flags()}
     del av, bias4

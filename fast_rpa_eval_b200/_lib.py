@@ -217,6 +217,15 @@ class Rho1Plan:
         check(lib().frpa_rho1_execute(self.handle, c_int(mode), c_int(n_active), _ptr(wave), _ptr(gwave), _ptr(P1),
                                       _ptr(bias), _ptr(gbias), _ptr(rho), _ptr(grad), _stream(stream)))
 
+    def execute_fused_bias(self, n_active, n_atoms, j_atom_begin, j_coord, atom_valid, density_matrix, wave, gwave,
+                           P1, bias, gbias, rho, grad, stream=None):
+        """frpa_rho1_execute_fused_bias: FP64 rho1 with the density-matrix bias
+        computed in the same launch."""
+        check(lib().frpa_rho1_execute_fused_bias(
+            self.handle, c_int(n_active), c_int(n_atoms), c_int(j_atom_begin), c_int(j_coord), _ptr(atom_valid),
+            _ptr(density_matrix), _ptr(wave), _ptr(gwave), _ptr(P1), _ptr(bias), _ptr(gbias), _ptr(rho), _ptr(grad),
+            _stream(stream)))
+
     def device_flags(self) -> int:
         f = c_int(0)
         check(lib().frpa_rho1_device_flags(self.handle, ctypes.byref(f)))

@@ -452,6 +452,24 @@ int frpa_rho1_execute(const frpa_rho1_plan *plan, int mode, int n_active, const 
   return rho1_run(*plan->p, mode, n_active, wave, gradient_wave, P1, bias, gbias, rho, grad, (cudaStream_t)stream);
 }
 
+int frpa_rho1_execute_fused_bias(const frpa_rho1_plan *plan, int n_active, int n_atoms, int j_atom_begin,
+                                 int j_coord, const int *atom_valid, const double *density_matrix, const double *wave,
+                                 const double *gradient_wave, const double *P1, const double *bias,
+                                 const double *gbias, double *rho, double *grad, void *stream) {
+  if (!plan) return fail(FRPA_ERR_INVALID, "rho1: null plan");
+  Rho1Plan &P = *plan->p;
+  FRPA_CHECK_ARG(P1 && bias && gbias && rho && grad && atom_valid && density_matrix, "rho1 fused bias: null pointer");
+  FRPA_CHECK_ARG(P.n_items == 0 || (wave && gradient_wave), "rho1 fused bias: null wave pointer");
+  FRPA_CHECK_ARG(n_active >= 0 && n_active <= P.T, "rho1 fused bias: n_active %d outside 0..%d", n_active, P.T);
+  FRPA_CHECK_ARG(j_coord >= 1 && j_coord <= 3, "rho1 fused bias: j_coord %d outside 1..3", j_coord);
+  FRPA_CHECK_ARG(n_active == 0 || (j_atom_begin >= 1 && j_atom_begin + n_active - 1 <= n_atoms),
+                 "rho1 fused bias: atoms %d..%d outside 1..%d", j_atom_begin, j_atom_begin + n_active - 1, n_atoms);
+  Rho1Plan Q = P;
+  if (((uintptr_t)wave | (uintptr_t)gradient_wave) & 15) Q.wave_aligned16 = 0;
+  return rho1_fp64_fused_bias_launch(Q, n_active, n_atoms, j_atom_begin, j_coord, atom_valid, density_matrix, wave,
+                                     gradient_wave, P1, bias, gbias, rho, grad, (cudaStream_t)stream);
+}
+
 int frpa_rho1_device_flags(const frpa_rho1_plan *plan, int *flags) {
   if (!plan || !flags) return fail(FRPA_ERR_INVALID, "rho1: null argument");
   FRPA_CUDA_TRY(cudaMemcpy(flags, plan->p->d_err, sizeof(int), cudaMemcpyDeviceToHost));

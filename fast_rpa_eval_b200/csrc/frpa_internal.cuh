@@ -205,6 +205,10 @@ int rho1_fp64_launch(const Rho1Plan &plan, int n_active, const double *wave, con
                      const double *P1, const double *bias, const double *gbias, double *rho, double *grad,
                      cudaStream_t stream);
 int rho1_fp64_grid(int device);
+int rho1_fp64_fused_bias_launch(const Rho1Plan &plan, int n_active, int n_atoms, int j_atom_begin, int j_coord,
+                                const int *atom_valid, const double *density_matrix, const double *wave,
+                                const double *gwave, const double *P1, const double *bias, const double *gbias,
+                                double *rho, double *grad, cudaStream_t stream);
 int rho1_split_launch(const Rho1Plan &plan, int n_active, const double *wave, const double *gwave,
                       const double *P1, const double *bias, const double *gbias, double *rho, double *grad,
                       cudaStream_t stream);

@@ -16,6 +16,15 @@
 // contracts each finished work1 tile against phi / grad phi, so work1 never
 // leaves the SM.  Per-point sums are reduced in a fixed order (registers ->
 // warp shuffles -> two shared-memory slots), so results are deterministic.
+//
+// Optionally the same launch also computes the ground-state density-matrix
+// part of the rho1 bias (what generate_first_order_rho_bias_part2.cpp:84-150
+// produces as a separate pass; the reference's fused form is
+// task1_atom_tiling/version3_rho_with_bias/evaluate_first_order_rho.cu.hpp:93-254):
+// for perturbation t = atom j_atom_begin + t with compute range R,
+//   bias(p) = sum_i phi_i(p) sum_{k in R} (D(ib_i, ib_k) + D(ib_k, ib_i)) (-d phi_k / d x_jcoord)(p),
+// as extra K chunks after each row tile's main chunks (A: the two gathers of
+// D, B: the gradient of phi along j_coord), added to rho1 only.
 #include <algorithm>
 #include <vector>
 
@@ -49,7 +58,17 @@ struct Smem {
   double B[STAGES][BN * LDB];
   double red[2][4][BN];
   int ib[MAX_NC];
+  int rs[FRPA_MAX_ATOM_TILE], re[FRPA_MAX_ATOM_TILE];  // fused bias: each perturbation's compute range
+  int nkb;                                             // fused bias: K chunks per row tile (both gathers)
   int next;
+};
+
+// The in-kernel bias inputs (null dm: no fused bias).
+struct FusedBias {
+  const double *dm;       // ground-state density matrix (n_basis, n_basis)
+  const int *atom_valid;  // (n_atoms + 1, n_batches), 0-based compute ranges
+  int n_atoms, j_atom_begin, j_coord;
+  int *err;               // device flags: bit 3 = a range leaves its batch (clipped)
 };
 
 template <int BN>
@@ -59,7 +78,7 @@ __global__ void __launch_bounds__(Fp64Shape<BN>::THREADS, Fp64Shape<BN>::MIN_BLO
                      int n_full_points, int n_max_batch_size, int n_batches, const double *__restrict__ wave,
                      const double *__restrict__ gwave, const double *__restrict__ P1,
                      const double *__restrict__ bias, const double *__restrict__ gbias, double *__restrict__ rho,
-                     double *__restrict__ grad, int aligned16) {
+                     double *__restrict__ grad, int aligned16, FusedBias fb) {
   constexpr int THREADS = Fp64Shape<BN>::THREADS, WN = Fp64Shape<BN>::WN;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   Smem<BN> &S = *reinterpret_cast<Smem<BN> *>(smem_raw);
@@ -78,22 +97,70 @@ __global__ void __launch_bounds__(Fp64Shape<BN>::THREADS, Fp64Shape<BN>::MIN_BLO
     const int nc = W.nc, pn = W.pn;
     const int ncp = (nc + 3) & ~3;
     for (int i = tid; i < nc; i += THREADS) S.ib[i] = ib_all[W.ib_off + i] - 1;
+    if (tid == 0) {
+      int rmax = 0;
+      for (int t = 0; t < T; ++t) {
+        int r0 = 0, r1 = 0;
+        if (fb.dm && t < n_active) {  // the bias of perturbation t belongs to atom j_atom_begin + t
+          const int atom = fb.j_atom_begin + t;
+          const int s0 = fb.atom_valid[(atom - 1) + (long long)(fb.n_atoms + 1) * W.batch];
+          const int s1 = fb.atom_valid[atom + (long long)(fb.n_atoms + 1) * W.batch];
+          r0 = min(max(s0, 0), nc);
+          r1 = min(max(s1, r0), nc);
+          if (r0 != s0 || r1 != s1) atomicOr(fb.err, 8);
+        }
+        S.rs[t] = r0;
+        S.re[t] = r1;
+        rmax = max(rmax, r1 - r0);
+      }
+      S.nkb = 2 * ((rmax + KC - 1) / KC);
+    }
     __syncthreads();
 
     const double *phi = wave + W.wave_off + (long long)W.p0 * ncp;
     const double *gph = gwave + 3 * W.wave_off + 3LL * W.p0 * ncp;
     const int nMt = (nc + BM - 1) / BM;
     const int nKc = (nc + KC - 1) / KC;
-    const int steps = T * nMt * nKc;
+    const int nKb = S.nkb, nKs = nKc + nKb;  // K chunks per (t, row tile): main, then the bias's
+    const int steps = T * nMt * nKs;
 
     auto load = [&](int s) {
-      const int kc = s % nKc;
-      const int rest = s / nKc;
+      const int kk = s % nKs;
+      const int rest = s / nKs;
       const int mt = rest % nMt;
       const int t = rest / nMt;
-      const int k0 = kc * KC, m0 = mt * BM;
+      const int m0 = mt * BM;
       double *As = S.A[s % STAGES];
       double *Bs = S.B[s % STAGES];
+      if (kk >= nKc) {
+        // bias chunk: first the gather D(ib_i, ib_k), then D(ib_k, ib_i), over
+        // k in the perturbation's range; B = d phi_k / d x_jcoord
+        const int b = kk - nKc, hb = nKb / 2, tr = b / hb;
+        const int k0 = S.rs[t] + (b % hb) * KC, kend = S.re[t];
+#pragma unroll
+        for (int j = 0; j < (BM * KC) / THREADS; ++j) {
+          const int e = tid + THREADS * j;
+          const int m = e & (BM - 1), k = e / BM;
+          const int gm = m0 + m, gk = k0 + k;
+          const bool ok = gm < nc && gk < kend;
+          const double *src =
+              ok ? fb.dm + (tr == 0 ? S.ib[gm] + (long long)S.ib[gk] * n_basis : S.ib[gk] + (long long)S.ib[gm] * n_basis)
+                 : fb.dm;
+          cp_async_8(&As[k * LDA + m], src, ok ? 8 : 0);
+        }
+#pragma unroll
+        for (int j = 0; j < (BN * KC) / THREADS; ++j) {
+          const int e = tid + THREADS * j;
+          const int k = e & (KC - 1), n = e / KC;
+          const int gk = k0 + k;
+          const bool ok = n < pn && gk < kend;
+          cp_async_8(&Bs[n * LDB + k], ok ? gph + gk + (long long)ncp * ((fb.j_coord - 1) + 3LL * n) : gph,
+                     ok ? 8 : 0);
+        }
+        return;
+      }
+      const int kc = kk;
+      const int k0 = kc * KC;
       const double *P = P1 + t * nb2;
 #pragma unroll
       for (int j = 0; j < (BM * KC) / THREADS; ++j) {
@@ -150,11 +217,12 @@ __global__ void __launch_bounds__(Fp64Shape<BN>::THREADS, Fp64Shape<BN>::MIN_BLO
       if (s + STAGES - 1 < steps) load(s + STAGES - 1);
       cp_async_commit();
 
-      const int kc = s % nKc;
-      const int rest = s / nKc;
+      const int kk = s % nKs;
+      const int rest = s / nKs;
       const int mt = rest % nMt;
       const int t = rest / nMt;
-      const int k0 = kc * KC, m0 = mt * BM;
+      const int kc = kk;
+      const int k0 = kk < nKc ? kc * KC : 0, m0 = mt * BM;
       const double *As = S.A[s % STAGES];
       const double *Bs = S.B[s % STAGES];
       const int row_w = m0 + wm * 32;
@@ -200,7 +268,23 @@ __global__ void __launch_bounds__(Fp64Shape<BN>::THREADS, Fp64Shape<BN>::MIN_BLO
 #pragma unroll
           for (int ni = 0; ni < 2; ++ni) acc[mi][ni][0] = acc[mi][ni][1] = 0.0;
         }
-
+      }
+      if (nKb > 0 && kk == nKs - 1) {
+        // the bias of this row tile: rho1 -= sum_i phi_i (S d phi / d x_jcoord)_i
+#pragma unroll
+        for (int mi = 0; mi < 4; ++mi) {
+          const int row = row_w + mi * 8 + g;
+#pragma unroll
+          for (int ni = 0; ni < 2; ++ni)
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+              const int col = col_w + ni * 8 + 2 * q + h;
+              if (row < nc && col < pn) s_r[ni][h] -= __ldg(phi + row + (long long)col * ncp) * acc[mi][ni][h];
+              acc[mi][ni][h] = 0.0;
+            }
+        }
+      }
+      if (kk == nKs - 1) {
         if (mt == nMt - 1) {
           // all rows of perturbation t done: reduce over rows and write
 #pragma unroll
@@ -276,14 +360,17 @@ int fp64_grid(int device, int ctas_per_sm) {
 
 template <int BN>
 int fp64_launch(const Rho1Plan &plan, int n_active, const double *wave, const double *gwave, const double *P1,
-                const double *bias, const double *gbias, double *rho, double *grad, cudaStream_t stream) {
+                const double *bias, const double *gbias, double *rho, double *grad, const FusedBias *fused,
+                cudaStream_t stream) {
   int grid = fp64_grid<BN>(plan.device, plan.fp64_ctas_per_sm);
   if (grid <= 0) return fail(FRPA_ERR_CUDA, "rho1_fp64: occupancy query failed");
   if (grid > plan.n_items) grid = plan.n_items;
+  FusedBias fb{};
+  if (fused) fb = *fused;
   rho1_fp64_kernel<BN><<<grid, Fp64Shape<BN>::THREADS, sizeof(Smem<BN>), stream>>>(
       plan.d_items, plan.n_items, plan.d_counter, plan.d_ib, plan.d_map, plan.T, n_active, plan.n_basis,
       plan.n_full_points, plan.n_max_batch_size, plan.n_batches, wave, gwave, P1, bias, gbias, rho, grad,
-      plan.wave_aligned16);
+      plan.wave_aligned16, fb);
   FRPA_LAUNCH_CHECK();
   return FRPA_OK;
 }
@@ -296,8 +383,9 @@ int rho1_fp64_grid(int device) {
   return fp64_grid<64>(device, 0) > 0 && fp64_grid<128>(device, 0) > 0 ? fp64_grid<64>(device, 0) : 0;
 }
 
-int rho1_fp64_launch(const Rho1Plan &plan, int n_active, const double *wave, const double *gwave, const double *P1,
-                     const double *bias, const double *gbias, double *rho, double *grad, cudaStream_t stream) {
+static int fp64_run(const Rho1Plan &plan, int n_active, const double *wave, const double *gwave, const double *P1,
+                    const double *bias, const double *gbias, double *rho, double *grad, const FusedBias *fused,
+                    cudaStream_t stream) {
   // evaluate_first_order_rho.cpp:113-114 zeroes both outputs before the batch loop
   FRPA_CUDA_TRY(cudaMemsetAsync(rho, 0, sizeof(double) * (size_t)plan.n_full_points * plan.T, stream));
   FRPA_CUDA_TRY(cudaMemsetAsync(
@@ -305,8 +393,21 @@ int rho1_fp64_launch(const Rho1Plan &plan, int n_active, const double *wave, con
   if (plan.n_items == 0) return FRPA_OK;
   FRPA_CUDA_TRY(cudaMemsetAsync(plan.d_counter, 0, sizeof(int), stream));
   if (plan.fp64_tile_points == 128)
-    return fp64_launch<128>(plan, n_active, wave, gwave, P1, bias, gbias, rho, grad, stream);
-  return fp64_launch<64>(plan, n_active, wave, gwave, P1, bias, gbias, rho, grad, stream);
+    return fp64_launch<128>(plan, n_active, wave, gwave, P1, bias, gbias, rho, grad, fused, stream);
+  return fp64_launch<64>(plan, n_active, wave, gwave, P1, bias, gbias, rho, grad, fused, stream);
+}
+
+int rho1_fp64_launch(const Rho1Plan &plan, int n_active, const double *wave, const double *gwave, const double *P1,
+                     const double *bias, const double *gbias, double *rho, double *grad, cudaStream_t stream) {
+  return fp64_run(plan, n_active, wave, gwave, P1, bias, gbias, rho, grad, nullptr, stream);
+}
+
+int rho1_fp64_fused_bias_launch(const Rho1Plan &plan, int n_active, int n_atoms, int j_atom_begin, int j_coord,
+                                const int *atom_valid, const double *density_matrix, const double *wave,
+                                const double *gwave, const double *P1, const double *bias, const double *gbias,
+                                double *rho, double *grad, cudaStream_t stream) {
+  FusedBias fb{density_matrix, atom_valid, n_atoms, j_atom_begin, j_coord, plan.d_err};
+  return fp64_run(plan, n_active, wave, gwave, P1, bias, gbias, rho, grad, &fb, stream);
 }
 
 // Work items of <= tile_points points (a batch's points split evenly, widths a

@@ -291,6 +291,21 @@ int frpa_rho1_execute(const frpa_rho1_plan *plan, int mode, int n_active, const 
                       const double *gradient_wave, const double *P1, const double *bias, const double *gbias,
                       double *rho, double *grad, void *stream);
 
+/* rho1 and grad rho1 as frpa_rho1_execute in the FP64 mode, with the
+ * ground-state density-matrix part of the rho1 bias computed in the same
+ * launch (the reference's fused form, task1_atom_tiling/version3_rho_with_bias/
+ * evaluate_first_order_rho.cu.hpp:93-254, instead of a separate
+ * generate_first_order_rho_bias_part2 pass): for perturbation t (atom
+ * j_atom_begin + t, compute range from atom_valid (n_atoms + 1, n_batches))
+ *   rho1 += sum_i phi_i sum_{k in range} (D(ib_i, ib_k) + D(ib_k, ib_i)) (-d phi_k / d x_jcoord),
+ * added to rho1 only (grad rho1 as frpa_rho1_execute); the bias array is still
+ * added as in frpa_rho1_execute.  density_matrix (n_basis, n_basis) and
+ * atom_valid are device arrays.  No counterpart name in the reference. */
+int frpa_rho1_execute_fused_bias(const frpa_rho1_plan *plan, int n_active, int n_atoms, int j_atom_begin,
+                                 int j_coord, const int *atom_valid, const double *density_matrix, const double *wave,
+                                 const double *gradient_wave, const double *P1, const double *bias,
+                                 const double *gbias, double *rho, double *grad, void *stream);
+
 /* The same bias on the device with a plan's work list: atom_valid
  * ((n_atoms + 1, n_batches), 0-based ranges as in the reference), wave,
  * gradient_wave, density_matrix (n_basis, n_basis) and the output

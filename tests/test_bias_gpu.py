@@ -81,3 +81,42 @@ def test_bias_flags_a_range_outside_the_batch():
                     dev(p.gradient_wave), dev(np.eye(p.n_basis)), out)
     torch.cuda.synchronize()
     assert plan.device_flags() & 8
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("j_coord", [1, 2])
+def test_fused_bias_equals_rho1_plus_bias_part2(j_coord):
+    """frpa_rho1_execute_fused_bias: rho1 with the density-matrix bias computed
+    in the same launch equals the two-launch form (rho1 plus the oracle's
+    bias part 2 for the active perturbations); grad rho1 is unchanged."""
+    import torch
+
+    from gpu_util import dev, host
+
+    p = synth.make_rho1_problem(T=4, seed=9, n_atoms=6, n_batches=24, pad_value=np.nan, n_active=3,
+                                with_bias=True)
+    p.j_atom_begin, p.j_atom_end = 2, 4
+    dm = np.random.default_rng(5).normal(size=(p.n_basis, p.n_basis))  # not symmetric: both gathers matter
+    plan = _lib.Rho1Plan(p)
+    args = [dev(p.wave), dev(p.gradient_wave), dev(p.first_order_density_matrix), dev(p.first_order_rho_bias_part2),
+            dev(p.first_order_gradient_rho_bias)]
+    n_rho, n_grad = p.n_full_points * 4, 3 * p.n_max_batch_size * p.n_my_batches_work * 4
+    rho, grad = (torch.zeros(n, dtype=torch.float64, device="cuda") for n in (n_rho, n_grad))
+    rho0, grad0 = (torch.zeros(n, dtype=torch.float64, device="cuda") for n in (n_rho, n_grad))
+    plan.execute_fused_bias(3, p.n_atoms, 2, j_coord, dev(p.atom_valid_n_compute_c_batches, np.int32), dev(dm),
+                            *args, rho, grad)
+    plan.execute(3, *args, rho0, grad0, mode=_lib.RHO1_FP64)
+    torch.cuda.synchronize()
+    assert plan.device_flags() == 0
+    bias2 = oracle.rho_bias_part2(p, dm, j_coord=j_coord)  # (nmb, nb, 4)
+    want = host(rho0, (p.n_full_points, 4)).copy()
+    pre, pmap = p.n_point_batches_prefix_sum, p.i_valid_point_2_i_full_points_map
+    for b in range(p.n_my_batches_work):
+        if p.n_compute_c_batches[b] <= 0:
+            continue
+        pts = pmap[pre[b]:pre[b + 1]]
+        want[pts, :3] += bias2[:len(pts), b, :3]
+    got = host(rho, (p.n_full_points, 4))
+    assert rel(got, want) < TOL
+    assert np.array_equal(got[:, 3], want[:, 3])  # perturbation 4 is not active
+    assert torch.equal(grad, grad0)
