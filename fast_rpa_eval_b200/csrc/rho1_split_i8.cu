@@ -162,31 +162,64 @@ __device__ __forceinline__ void ld4(const double *p, double *v) {
 }
 
 constexpr int PA_THREADS = 256;
-constexpr int PA_GROUP = 16;  // points per pass: their rows are re-read from L2, not DRAM
+constexpr int PA_GROUP = 8;  // points per pass: one 8-row group of the tile image
+
+// Shared-memory row layout of pack A: 16-value pieces padded to 17 doubles
+// and rows padded to 4 (mod 16) doubles, so that the 32 threads of a warp
+// reading one value of 8 rows x 4 pieces hit distinct bank pairs.
+__host__ __device__ __forceinline__ int pa_row_stride(int kpad) {
+  const int ldr = (kpad / 16) * 17;
+  return ldr + ((4 - ldr) % 16 + 16) % 16;
+}
 
 // phi of one work item -> A scratch: chunk kc, plane s at
 // a_off + (5 kc + s) rows8 32 bytes; rows pn..rows8-1 and k >= nc are zero.
-// Sixteen points at a time: their scales (one warp per point, lanes along the
-// row), then their digits (one thread per row and 16-wide K group; a warp's
-// stores cover 512 contiguous bytes of a plane).
+// Eight points at a time: one warp per point copies its row into shared
+// memory (lanes along the row, 256-bit loads when rows are 32-byte aligned)
+// and finds its scale on the way, then every thread turns 16-wide K pieces of
+// the staged rows into five 16-byte digit planes (a warp's stores cover whole
+// 128-byte core-matrix rows).  phi crosses HBM once.
 __global__ void __launch_bounds__(PA_THREADS) i8_pack_a_kernel(const I8Item *__restrict__ items,
                                                                const double *__restrict__ wave,
                                                                unsigned char *__restrict__ a_scr,
                                                                double *__restrict__ sa, int vec) {
+  extern __shared__ __align__(32) double s_rows[];  // PA_GROUP rows, pa_row_stride(kpad) doubles each
   __shared__ double s_sc[PA_GROUP];
   const I8Item W = items[blockIdx.x];
-  const int nc = W.nc, pn = W.pn, rows8 = W.rows8, ncp = (nc + 3) & ~3;
+  const int nc = W.nc, pn = W.pn, rows8 = W.rows8, ncp = (nc + 3) & ~3, kpad = W.n_kc * I8_KC;
+  const int ld = pa_row_stride(kpad);
   const double *phi = wave + W.wave_off + (long long)W.p0 * ncp;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const long long chunk = (long long)I8_SLICES * rows8 * I8_ROWB;
   for (int g0 = 0; g0 < rows8; g0 += PA_GROUP) {
-    const int gn = min(PA_GROUP, rows8 - g0);  // 8 or 16
-    for (int r = warp; r < gn; r += PA_THREADS / 32) {
-      const int p = g0 + r;
+    {  // warp r stages row g0 + r (zeros past n_compute and for padding rows)
+      const int r = warp, p = g0 + r;
+      double *dst = s_rows + r * ld;
+      auto at = [](int k) { return (k >> 4) * 17 + (k & 15); };
       double m = 0.0;
       if (p < pn) {
         const double *row = phi + (long long)p * ncp;
-        for (int k = lane; k < nc; k += 32) m = fmax(m, fabs(__ldg(row + k)));
+        if (vec) {  // rows start on 32-byte boundaries; a vector that starts below nc ends by ncp
+          for (int k = 4 * lane; k < nc; k += 128) {
+            double v[4];
+            ld4(row + k, v);
+#pragma unroll
+            for (int e = 0; e < 4; ++e) {
+              const double x = k + e < nc ? v[e] : 0.0;
+              dst[at(k) + e] = x;
+              m = fmax(m, fabs(x));
+            }
+          }
+          for (int k = ((nc + 3) & ~3) + lane; k < kpad; k += 32) dst[at(k)] = 0.0;
+        } else {
+          for (int k = lane; k < kpad; k += 32) {
+            const double x = k < nc ? __ldg(row + k) : 0.0;
+            dst[at(k)] = x;
+            m = fmax(m, fabs(x));
+          }
+        }
+      } else {
+        for (int k = lane; k < kpad; k += 32) dst[at(k)] = 0.0;
       }
 #pragma unroll
       for (int o = 16; o; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
@@ -194,39 +227,24 @@ __global__ void __launch_bounds__(PA_THREADS) i8_pack_a_kernel(const I8Item *__r
         double sc39, s23;
         digit_scale(m, &sc39, &s23);
         s_sc[r] = sc39;
-        sa[W.sa_off + p] = s23;
+        if (p < pn) sa[W.sa_off + p] = s23;
       }
     }
     __syncthreads();
-    const int units = W.n_kc * 2 * gn;
+    const int units = W.n_kc * 2 * PA_GROUP;
     for (int u = threadIdx.x; u < units; u += PA_THREADS) {
-      const int r = u % gn, kg = (u / gn) & 1, kc = u / (2 * gn), p = g0 + r;
-      const int k0 = kc * I8_KC + kg * 16;
-      const double *row = phi + (long long)(p < pn ? p : 0) * ncp;
+      const int r = u % PA_GROUP, kg = (u / PA_GROUP) & 1, kc = u / (2 * PA_GROUP), p = g0 + r;
+      const double *src = s_rows + r * ld + (2 * kc + kg) * 17;
       double x[16];
-      if (vec) {  // rows start on 32-byte boundaries; a vector that starts below nc ends by ncp
 #pragma unroll
-        for (int v = 0; v < 4; ++v) {
-          if (p < pn && k0 + 4 * v < nc) {
-            ld4(row + k0 + 4 * v, &x[4 * v]);
-          } else {
-#pragma unroll
-            for (int e = 0; e < 4; ++e) x[4 * v + e] = 0.0;
-          }
-        }
-#pragma unroll
-        for (int j = 0; j < 16; ++j) x[j] = k0 + j < nc ? x[j] : 0.0;  // the row padding
-      } else {
-#pragma unroll
-        for (int j = 0; j < 16; ++j) x[j] = (p < pn && k0 + j < nc) ? __ldg(row + k0 + j) : 0.0;
-      }
+      for (int j = 0; j < 16; ++j) x[j] = src[j];
       uint4 plane[I8_SLICES];
       digits16(x, s_sc[r], plane);
       unsigned char *dst = a_scr + W.a_off + kc * chunk + plane_off(p, kg);
 #pragma unroll
       for (int s = 0; s < I8_SLICES; ++s) *reinterpret_cast<uint4 *>(dst + s * rows8 * I8_ROWB) = plane[s];
     }
-    __syncthreads();  // s_sc is rewritten by the next group
+    __syncthreads();  // the rows and scales are rewritten by the next group
   }
 }
 
@@ -758,8 +776,13 @@ int rho1_i8_launch(Rho1Plan &plan, int n_active, const double *wave, const doubl
   FRPA_TRY(p1_rowmax_launch(plan, P1, stream));
   static PerDeviceOnce configured;
   const int smem = i8_smem_bytes();
-  FRPA_TRY(configured.run(plan.device, [smem]() -> int {
+  // pack A stages PA_GROUP rows of up to n_compute (rounded to a K chunk) doubles
+  const int pa_smem =
+      (int)sizeof(double) * PA_GROUP * pa_row_stride(ceil_div(std::max(1, plan.n_max_compute), I8_KC) * I8_KC);
+  const int PA_SMEM_MAX = (int)sizeof(double) * PA_GROUP * pa_row_stride(FRPA_MAX_N_COMPUTE);
+  FRPA_TRY(configured.run(plan.device, [smem, PA_SMEM_MAX]() -> int {
     FRPA_CUDA_TRY(cudaFuncSetAttribute(rho1_i8_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    FRPA_CUDA_TRY(cudaFuncSetAttribute(i8_pack_a_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, PA_SMEM_MAX));
     return FRPA_OK;
   }));
   int n_sm = 148;
@@ -787,8 +810,8 @@ int rho1_i8_launch(Rho1Plan &plan, int n_active, const double *wave, const doubl
   P.sa = plan.d_i8_sa;
   for (const I8Group &g : plan.i8_groups) {
     const int ni = g.item1 - g.item0, nu = g.unit1 - g.unit0;
-    i8_pack_a_kernel<<<ni, PA_THREADS, 0, stream>>>(plan.d_i8_items + g.item0, wave, plan.d_i8_a, plan.d_i8_sa,
-                                                    P.wave_vec);
+    i8_pack_a_kernel<<<ni, PA_THREADS, pa_smem, stream>>>(plan.d_i8_items + g.item0, wave, plan.d_i8_a,
+                                                          plan.d_i8_sa, P.wave_vec);
     FRPA_LAUNCH_CHECK();
     P.items = plan.d_i8_items;
     P.units = plan.d_i8_units + g.unit0;
