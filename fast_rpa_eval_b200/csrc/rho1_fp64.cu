@@ -45,11 +45,12 @@ constexpr int MAX_NC = FRPA_MAX_N_COMPUTE;
 // 50 KB of shared memory each; measured faster than 2 CTAs with deeper
 // rings); BN = 128: 512 threads, one CTA per SM, each gathered P1c tile
 // serving twice the points.
-template <int BN>
+template <int BN, bool BIAS>
 struct Fp64Shape {
   static constexpr int WN = BN / 16;
   static constexpr int THREADS = 64 * WN;
-  static constexpr int MIN_BLOCKS = BN == 64 ? 3 : 1;
+  // the fused-bias form carries more state: two CTAs per SM instead of three
+  static constexpr int MIN_BLOCKS = BN == 64 ? (BIAS ? 2 : 3) : 1;
 };
 
 template <int BN>
@@ -71,15 +72,15 @@ struct FusedBias {
   int *err;               // device flags: bit 3 = a range leaves its batch (clipped)
 };
 
-template <int BN>
-__global__ void __launch_bounds__(Fp64Shape<BN>::THREADS, Fp64Shape<BN>::MIN_BLOCKS)
+template <int BN, bool BIAS>
+__global__ void __launch_bounds__(Fp64Shape<BN, BIAS>::THREADS, Fp64Shape<BN, BIAS>::MIN_BLOCKS)
     rho1_fp64_kernel(const Rho1WorkItem *__restrict__ items, int n_items, int *__restrict__ counter,
                      const int *__restrict__ ib_all, const int *__restrict__ map, int T, int n_active, int n_basis,
                      int n_full_points, int n_max_batch_size, int n_batches, const double *__restrict__ wave,
                      const double *__restrict__ gwave, const double *__restrict__ P1,
                      const double *__restrict__ bias, const double *__restrict__ gbias, double *__restrict__ rho,
                      double *__restrict__ grad, int aligned16, FusedBias fb) {
-  constexpr int THREADS = Fp64Shape<BN>::THREADS, WN = Fp64Shape<BN>::WN;
+  constexpr int THREADS = Fp64Shape<BN, BIAS>::THREADS, WN = Fp64Shape<BN, BIAS>::WN;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   Smem<BN> &S = *reinterpret_cast<Smem<BN> *>(smem_raw);
   const int tid = threadIdx.x;
@@ -97,7 +98,7 @@ __global__ void __launch_bounds__(Fp64Shape<BN>::THREADS, Fp64Shape<BN>::MIN_BLO
     const int nc = W.nc, pn = W.pn;
     const int ncp = (nc + 3) & ~3;
     for (int i = tid; i < nc; i += THREADS) S.ib[i] = ib_all[W.ib_off + i] - 1;
-    if (tid == 0) {
+    if (BIAS && tid == 0) {
       int rmax = 0;
       for (int t = 0; t < T; ++t) {
         int r0 = 0, r1 = 0;
@@ -121,7 +122,7 @@ __global__ void __launch_bounds__(Fp64Shape<BN>::THREADS, Fp64Shape<BN>::MIN_BLO
     const double *gph = gwave + 3 * W.wave_off + 3LL * W.p0 * ncp;
     const int nMt = (nc + BM - 1) / BM;
     const int nKc = (nc + KC - 1) / KC;
-    const int nKb = S.nkb, nKs = nKc + nKb;  // K chunks per (t, row tile): main, then the bias's
+    const int nKb = BIAS ? S.nkb : 0, nKs = nKc + nKb;  // K chunks per (t, row tile): main, then the bias's
     const int steps = T * nMt * nKs;
 
     auto load = [&](int s) {
@@ -132,7 +133,7 @@ __global__ void __launch_bounds__(Fp64Shape<BN>::THREADS, Fp64Shape<BN>::MIN_BLO
       const int m0 = mt * BM;
       double *As = S.A[s % STAGES];
       double *Bs = S.B[s % STAGES];
-      if (kk >= nKc) {
+      if (BIAS && kk >= nKc) {
         // bias chunk: first the gather D(ib_i, ib_k), then D(ib_k, ib_i), over
         // k in the perturbation's range; B = d phi_k / d x_jcoord
         const int b = kk - nKc, hb = nKb / 2, tr = b / hb;
@@ -211,6 +212,54 @@ __global__ void __launch_bounds__(Fp64Shape<BN>::THREADS, Fp64Shape<BN>::MIN_BLO
       cp_async_commit();
     }
 
+    // all rows of perturbation t done: reduce the per-point sums over rows,
+    // write rho1 and grad rho1, clear the sums
+    auto finish = [&](int t) {
+#pragma unroll
+      for (int ni = 0; ni < 2; ++ni)
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+#pragma unroll
+          for (int off = 4; off < 32; off <<= 1) {
+            s_r[ni][h] += __shfl_xor_sync(0xffffffffu, s_r[ni][h], off);
+            s_x[ni][h] += __shfl_xor_sync(0xffffffffu, s_x[ni][h], off);
+            s_y[ni][h] += __shfl_xor_sync(0xffffffffu, s_y[ni][h], off);
+            s_z[ni][h] += __shfl_xor_sync(0xffffffffu, s_z[ni][h], off);
+          }
+        }
+      if (g == 0) {
+#pragma unroll
+        for (int ni = 0; ni < 2; ++ni)
+#pragma unroll
+          for (int h = 0; h < 2; ++h) {
+            const int col = wn * 16 + ni * 8 + 2 * q + h;
+            S.red[wm][0][col] = s_r[ni][h];
+            S.red[wm][1][col] = s_x[ni][h];
+            S.red[wm][2][col] = s_y[ni][h];
+            S.red[wm][3][col] = s_z[ni][h];
+          }
+      }
+      __syncthreads();
+      if (tid < pn) {
+        const int p = W.p0 + tid;
+        const double r = S.red[0][0][tid] + S.red[1][0][tid];
+        const double gx = S.red[0][1][tid] + S.red[1][1][tid];
+        const double gy = S.red[0][2][tid] + S.red[1][2][tid];
+        const double gz = S.red[0][3][tid] + S.red[1][3][tid];
+        const long long bidx = p + (long long)n_max_batch_size * (W.batch + (long long)n_batches * t);
+        const long long gi = 3 * bidx;
+        grad[gi + 0] = gx * 2 - gbias[gi + 0];
+        grad[gi + 1] = gy * 2 - gbias[gi + 1];
+        grad[gi + 2] = gz * 2 - gbias[gi + 2];
+        if (t < n_active) rho[map[W.prefix + p] + (long long)n_full_points * t] = r + bias[bidx];
+      }
+#pragma unroll
+      for (int ni = 0; ni < 2; ++ni)
+#pragma unroll
+        for (int h = 0; h < 2; ++h) s_r[ni][h] = s_x[ni][h] = s_y[ni][h] = s_z[ni][h] = 0.0;
+      __syncthreads();
+    };
+
     for (int s = 0; s < steps; ++s) {
       cp_async_wait<STAGES - 2>();
       __syncthreads();
@@ -222,7 +271,7 @@ __global__ void __launch_bounds__(Fp64Shape<BN>::THREADS, Fp64Shape<BN>::MIN_BLO
       const int mt = rest % nMt;
       const int t = rest / nMt;
       const int kc = kk;
-      const int k0 = kk < nKc ? kc * KC : 0, m0 = mt * BM;
+      const int k0 = (!BIAS || kk < nKc) ? kc * KC : 0, m0 = mt * BM;
       const double *As = S.A[s % STAGES];
       const double *Bs = S.B[s % STAGES];
       const int row_w = m0 + wm * 32;
@@ -268,8 +317,9 @@ __global__ void __launch_bounds__(Fp64Shape<BN>::THREADS, Fp64Shape<BN>::MIN_BLO
 #pragma unroll
           for (int ni = 0; ni < 2; ++ni) acc[mi][ni][0] = acc[mi][ni][1] = 0.0;
         }
+        if (!BIAS && mt == nMt - 1) finish(t);
       }
-      if (nKb > 0 && kk == nKs - 1) {
+      if (BIAS && nKb > 0 && kk == nKs - 1) {
         // the bias of this row tile: rho1 -= sum_i phi_i (S d phi / d x_jcoord)_i
 #pragma unroll
         for (int mi = 0; mi < 4; ++mi) {
@@ -284,69 +334,22 @@ __global__ void __launch_bounds__(Fp64Shape<BN>::THREADS, Fp64Shape<BN>::MIN_BLO
             }
         }
       }
-      if (kk == nKs - 1) {
-        if (mt == nMt - 1) {
-          // all rows of perturbation t done: reduce over rows and write
-#pragma unroll
-          for (int ni = 0; ni < 2; ++ni)
-#pragma unroll
-            for (int h = 0; h < 2; ++h) {
-#pragma unroll
-              for (int off = 4; off < 32; off <<= 1) {
-                s_r[ni][h] += __shfl_xor_sync(0xffffffffu, s_r[ni][h], off);
-                s_x[ni][h] += __shfl_xor_sync(0xffffffffu, s_x[ni][h], off);
-                s_y[ni][h] += __shfl_xor_sync(0xffffffffu, s_y[ni][h], off);
-                s_z[ni][h] += __shfl_xor_sync(0xffffffffu, s_z[ni][h], off);
-              }
-            }
-          if (g == 0) {
-#pragma unroll
-            for (int ni = 0; ni < 2; ++ni)
-#pragma unroll
-              for (int h = 0; h < 2; ++h) {
-                const int col = col_w + ni * 8 + 2 * q + h;
-                S.red[wm][0][col] = s_r[ni][h];
-                S.red[wm][1][col] = s_x[ni][h];
-                S.red[wm][2][col] = s_y[ni][h];
-                S.red[wm][3][col] = s_z[ni][h];
-              }
-          }
-          __syncthreads();
-          if (tid < pn) {
-            const int p = W.p0 + tid;
-            const double r = S.red[0][0][tid] + S.red[1][0][tid];
-            const double gx = S.red[0][1][tid] + S.red[1][1][tid];
-            const double gy = S.red[0][2][tid] + S.red[1][2][tid];
-            const double gz = S.red[0][3][tid] + S.red[1][3][tid];
-            const long long bidx = p + (long long)n_max_batch_size * (W.batch + (long long)n_batches * t);
-            const long long gi = 3 * bidx;
-            grad[gi + 0] = gx * 2 - gbias[gi + 0];
-            grad[gi + 1] = gy * 2 - gbias[gi + 1];
-            grad[gi + 2] = gz * 2 - gbias[gi + 2];
-            if (t < n_active) rho[map[W.prefix + p] + (long long)n_full_points * t] = r + bias[bidx];
-          }
-#pragma unroll
-          for (int ni = 0; ni < 2; ++ni)
-#pragma unroll
-            for (int h = 0; h < 2; ++h) s_r[ni][h] = s_x[ni][h] = s_y[ni][h] = s_z[ni][h] = 0.0;
-          __syncthreads();
-        }
-      }
+      if (BIAS && kk == nKs - 1 && mt == nMt - 1) finish(t);
     }
     cp_async_wait<0>();
     __syncthreads();
   }
 }
 
-template <int BN>
+template <int BN, bool BIAS>
 int fp64_grid(int device, int ctas_per_sm) {
   static int cached[64] = {0};
   const int smem = (int)sizeof(Smem<BN>);
   if (device < 0 || device >= 64 || !cached[device]) {
-    if (cudaFuncSetAttribute(rho1_fp64_kernel<BN>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) != cudaSuccess)
+    if (cudaFuncSetAttribute(rho1_fp64_kernel<BN, BIAS>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) != cudaSuccess)
       return 0;
     int per_sm = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, rho1_fp64_kernel<BN>, Fp64Shape<BN>::THREADS, smem) !=
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, rho1_fp64_kernel<BN, BIAS>, Fp64Shape<BN, BIAS>::THREADS, smem) !=
         cudaSuccess)
       return 0;
     if (device >= 0 && device < 64) cached[device] = per_sm > 0 ? per_sm : 1;
@@ -358,16 +361,16 @@ int fp64_grid(int device, int ctas_per_sm) {
   return per_sm * n_sm;
 }
 
-template <int BN>
+template <int BN, bool BIAS>
 int fp64_launch(const Rho1Plan &plan, int n_active, const double *wave, const double *gwave, const double *P1,
                 const double *bias, const double *gbias, double *rho, double *grad, const FusedBias *fused,
                 cudaStream_t stream) {
-  int grid = fp64_grid<BN>(plan.device, plan.fp64_ctas_per_sm);
+  int grid = fp64_grid<BN, BIAS>(plan.device, plan.fp64_ctas_per_sm);
   if (grid <= 0) return fail(FRPA_ERR_CUDA, "rho1_fp64: occupancy query failed");
   if (grid > plan.n_items) grid = plan.n_items;
   FusedBias fb{};
   if (fused) fb = *fused;
-  rho1_fp64_kernel<BN><<<grid, Fp64Shape<BN>::THREADS, sizeof(Smem<BN>), stream>>>(
+  rho1_fp64_kernel<BN, BIAS><<<grid, Fp64Shape<BN, BIAS>::THREADS, sizeof(Smem<BN>), stream>>>(
       plan.d_items, plan.n_items, plan.d_counter, plan.d_ib, plan.d_map, plan.T, n_active, plan.n_basis,
       plan.n_full_points, plan.n_max_batch_size, plan.n_batches, wave, gwave, P1, bias, gbias, rho, grad,
       plan.wave_aligned16, fb);
@@ -380,7 +383,10 @@ int fp64_launch(const Rho1Plan &plan, int n_active, const double *wave, const do
 // Sets the kernels' shared-memory attributes once per device (outside any
 // stream capture); 0 on failure.
 int rho1_fp64_grid(int device) {
-  return fp64_grid<64>(device, 0) > 0 && fp64_grid<128>(device, 0) > 0 ? fp64_grid<64>(device, 0) : 0;
+  return fp64_grid<64, false>(device, 0) > 0 && fp64_grid<128, false>(device, 0) > 0 &&
+                 fp64_grid<64, true>(device, 0) > 0 && fp64_grid<128, true>(device, 0) > 0
+             ? fp64_grid<64, false>(device, 0)
+             : 0;
 }
 
 static int fp64_run(const Rho1Plan &plan, int n_active, const double *wave, const double *gwave, const double *P1,
@@ -392,9 +398,14 @@ static int fp64_run(const Rho1Plan &plan, int n_active, const double *wave, cons
       grad, 0, sizeof(double) * 3 * (size_t)plan.n_max_batch_size * plan.n_batches * plan.T, stream));
   if (plan.n_items == 0) return FRPA_OK;
   FRPA_CUDA_TRY(cudaMemsetAsync(plan.d_counter, 0, sizeof(int), stream));
+  if (fused) {
+    if (plan.fp64_tile_points == 128)
+      return fp64_launch<128, true>(plan, n_active, wave, gwave, P1, bias, gbias, rho, grad, fused, stream);
+    return fp64_launch<64, true>(plan, n_active, wave, gwave, P1, bias, gbias, rho, grad, fused, stream);
+  }
   if (plan.fp64_tile_points == 128)
-    return fp64_launch<128>(plan, n_active, wave, gwave, P1, bias, gbias, rho, grad, fused, stream);
-  return fp64_launch<64>(plan, n_active, wave, gwave, P1, bias, gbias, rho, grad, fused, stream);
+    return fp64_launch<128, false>(plan, n_active, wave, gwave, P1, bias, gbias, rho, grad, nullptr, stream);
+  return fp64_launch<64, false>(plan, n_active, wave, gwave, P1, bias, gbias, rho, grad, nullptr, stream);
 }
 
 int rho1_fp64_launch(const Rho1Plan &plan, int n_active, const double *wave, const double *gwave, const double *P1,

@@ -319,16 +319,20 @@ __device__ void producer_role(const I8Params &P, I8Smem &S, int pw, int lane) {
       const int kcol = kc * I8_KC + lane;
       const int my_col = kcol < nc ? __ldg(ib + kcol) - 1 : -1;
       unsigned char *dst = S.B[slot];
+      // all 32 gathers of the row are issued before any is used: one memory
+      // round trip per chunk
+      double x[2][16];
 #pragma unroll
-      for (int kg = 0; kg < 2; ++kg) {
-        double x[16];
+      for (int kg = 0; kg < 2; ++kg)
 #pragma unroll
         for (int j = 0; j < 16; ++j) {
           const int col = __shfl_sync(0xffffffffu, my_col, kg * 16 + j);
-          x[j] = (rok && col >= 0) ? __ldg(P1t + ibr + (long long)col * P.n_basis) : 0.0;
+          x[kg][j] = (rok && col >= 0) ? __ldg(P1t + ibr + (long long)col * P.n_basis) : 0.0;
         }
+#pragma unroll
+      for (int kg = 0; kg < 2; ++kg) {
         uint4 plane[I8_SLICES];
-        digits16(x, sc39, plane);
+        digits16(x[kg], sc39, plane);
 #pragma unroll
         for (int s = 0; s < I8_SLICES; ++s)
           *reinterpret_cast<uint4 *>(dst + s * I8_N * I8_ROWB + plane_off(lane, kg)) = plane[s];

@@ -43,17 +43,18 @@ def test_cxx_linkage_symbols_resolve_in_the_library():
 @pytest.mark.gpu
 def test_session_through_cxx_linkage_matches_oracle():
     r = synth.make_rho1_problem(T=1, seed=13, n_batches=10, with_bias=True)
-    p = synth.make_sumup_problem(n_atoms=12, n_points=1200, l_pot_max=6, T=1, seed=84)
-    # one full-point set for both paths, as the session holds both
+    n_r = int(r.n_point_batches_prefix_sum[-1])
+    p = synth.make_sumup_problem(n_atoms=12, n_points=n_r + 800, l_pot_max=6, T=1, seed=84)
+    # the session holds one full-point set and one valid-point map for both
+    # paths (as init_dfpt_device_data does): rho1's points are the first n_r
+    # entries of the sum-up's map
     p.n_full_points = r.n_full_points = max(r.n_full_points, p.n_full_points)
     pad = p.n_full_points - p.coord_points.shape[1]
     p.coord_points = np.asfortranarray(np.concatenate([p.coord_points, np.zeros((3, pad))], axis=1))
     p.delta_v_hartree = np.asfortranarray(np.concatenate([p.delta_v_hartree, np.zeros((pad, 1))], axis=0))
     p.partition_tab = np.concatenate([p.partition_tab, np.ones(pad)])
     r.partition_tab = p.partition_tab
-    r.i_valid_point_2_i_full_points_map = np.concatenate(
-        [r.i_valid_point_2_i_full_points_map,
-         np.arange(len(r.i_valid_point_2_i_full_points_map), p.n_full_points)]).astype(np.int32)
+    r.i_valid_point_2_i_full_points_map = p.i_valid_point_2_i_full_points_map[:n_r].astype(np.int32).copy()
     with _lib.Session(r, p, entry=_entry()) as s:
         rho, grad = s.rho1()
         r_o, g_o = oracle.rho1(r)
