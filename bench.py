@@ -582,8 +582,7 @@ def run_frpa(args, ranks: Ranks):
     i8_traffic = profile_traffic("rho1_split_i8_step", p.n_my_batches_work)
     out["rho1_split_i8"] = {
         "pts_per_s": total_pts / (ms_i8 / 1e3), "ms_per_step": ms_i8, "speedup_vs_fp64": ms_fp64 / ms_i8,
-        "kernels_per_group": "pack A (phi digits), tcgen05.mma.kind::i8 contraction with P1c digits built in "
-                             "shared memory",
+        "kernels_per_group": "pack A (phi digits), pack B (P1c digits), tcgen05.mma.kind::i8 contraction",
         "groups": i8_groups,
         # roofline: the path's algorithmic bytes over the step time, against the
         # measured copy bandwidth; the DRAM bytes it actually moved (ncu, scaled
@@ -727,7 +726,7 @@ def run_frpa(args, ranks: Ranks):
         gbs = w_bytes / (ms / 1e3) / 1e9
         roofline = {"bound": "hbm", "achieved": gbs, "peak": peaks["hbm_gbs"], "unit": "GB/s",
                     "frac": gbs / peaks["hbm_gbs"], "traffic": traffic,
-                    "kernel": "split-int8 step (i8_pack_a_kernel, rho1_i8_kernel per group)",
+                    "kernel": "split-int8 step (i8_pack_a_kernel, i8_pack_b_kernel, rho1_i8_kernel per group)",
                     "achieved_from": "algorithmic bytes of the step (phi, grad phi, P1c once per batch, outputs) "
                                      "over the CUDA-event time",
                     "peak_source": peaks["source"] + " (MEASURED_PEAKS.json hbm_gbs)",
@@ -755,7 +754,7 @@ def run_frpa(args, ranks: Ranks):
                    "path": mode_name, "valid_batches": info["n_valid_batches"], "work_items": n_items_tuned,
                    "launch": ("one persistent grouped launch per step, replayed from a CUDA graph"
                               if mode != _lib.RHO1_SPLIT_I8 else
-                              f"row max + {i8_groups} groups x (pack phi, contraction), "
+                              f"row max + {i8_groups} groups x (pack phi, pack P1c, contraction), "
                               "replayed from a CUDA graph"),
                    "tuning": tuned or "defaults (--no-tune)",
                    "grid_points_per_rank": w_points,
@@ -766,7 +765,7 @@ def run_frpa(args, ranks: Ranks):
         "roofline": roofline,
         "clocks": clk,
         "gpu_launches": args.steps * {_lib.RHO1_FP64: 1, _lib.RHO1_SPLIT_BF16: 2,
-                                      _lib.RHO1_SPLIT_I8: 1 + 2 * i8_groups}[mode],
+                                      _lib.RHO1_SPLIT_I8: 1 + 3 * i8_groups}[mode],
         "cpu_baseline": cpu,
         "e2e": e2e,
         "measured_fp64_tflops": {"mma": fp64_peak, "fma": fma_peak},

@@ -207,11 +207,11 @@ class Rho1Plan:
         return {"n_items": out[0], "n_valid_batches": out[1], "n_valid_points": out[2]}
 
     def i8_info(self):
-        """Split-int8 grouping: groups (two launches each), point tiles,
-        contraction units, largest per-group packed-phi scratch in bytes."""
+        """Split-int8 grouping: groups (three launches each), work items,
+        packed P1c tiles, largest per-group A + B scratch in bytes."""
         out = (c_ll * 4)()
         check(lib().frpa_rho1_plan_i8_info(self.handle, out))
-        return {"groups": out[0], "items": out[1], "units": out[2], "scratch_bytes": out[3]}
+        return {"groups": out[0], "items": out[1], "b_tiles": out[2], "scratch_bytes": out[3]}
 
     def execute(self, n_active, wave, gwave, P1, bias, gbias, rho, grad, mode=RHO1_FP64, stream=None):
         check(lib().frpa_rho1_execute(self.handle, c_int(mode), c_int(n_active), _ptr(wave), _ptr(gwave), _ptr(P1),

@@ -432,15 +432,15 @@ int frpa_rho1_plan_info(const frpa_rho1_plan *plan, long long *info3) {
 int frpa_rho1_plan_i8_info(const frpa_rho1_plan *plan, long long *info4) {
   if (!plan || !info4) return fail(FRPA_ERR_INVALID, "rho1: null argument");
   const Rho1Plan &P = *plan->p;
-  long long items = 0, units = 0, scratch = 0;
+  long long items = 0, tiles = 0, scratch = 0;
   for (const I8Group &g : P.i8_groups) {
     items += g.item1 - g.item0;
-    units += g.unit1 - g.unit0;
-    scratch = std::max(scratch, g.a_bytes);
+    tiles += g.tile1 - g.tile0;
+    scratch = std::max(scratch, g.a_bytes + g.b_bytes);
   }
   info4[0] = (long long)P.i8_groups.size();
   info4[1] = items;
-  info4[2] = units;
+  info4[2] = tiles;
   info4[3] = scratch;
   return FRPA_OK;
 }

@@ -117,33 +117,38 @@ struct Rho1WorkItem {
 };
 static_assert(sizeof(Rho1WorkItem) == 40, "work item layout");
 
-// Split-int8 rho1 (rho1_split_i8.cu).  A work item is a point tile (<= 128
-// points) of one batch; the pack kernel writes its phi digits to the A
-// scratch.  A unit is up to three consecutive items of one batch for one
-// perturbation: one CTA contracts it, building the batch's P1c digits in
-// shared memory once for all of the unit's items.  Offsets are relative to
-// the scratch of the item's group (groups of batches are packed and
-// contracted in turn, so the scratch holds one group at a time).
+// Split-int8 rho1 (rho1_split_i8.cu).  A work item is a point tile of one
+// batch; its phi digits live in the A scratch, the batch's P1c digits (per
+// perturbation) in the B scratch.  Offsets are relative to the scratch of
+// the item's group: groups of consecutive batches are packed and contracted
+// in turn, so the scratch holds one group at a time.
 struct I8Item {
   int batch, nc, p0, pn;
-  int prefix, rows8, n_kc, sa_off;  // rows8 = pn rounded up to 8; K chunks of 32
+  int prefix, rows8, n_nt, n_kc;  // rows8 = pn rounded up to 8; N tiles of 32 rows; K chunks of 32
   long long wave_off;
-  long long a_off;  // bytes of the item's first A chunk
+  long long a_off;       // bytes of the item's first A chunk
+  long long b_off;       // bytes of the batch's first B chunk (t = 0)
+  long long b_tstride;   // B bytes per perturbation
+  int sa_off;            // first per-point scale of the item
+  int sb_off;            // first per-row scale of the batch (t = 0)
+  int sb_tstride;        // per-row scales per perturbation (n_nt * 32)
+  int pad_;
 };
-static_assert(sizeof(I8Item) == 48, "I8Item layout");
+static_assert(sizeof(I8Item) == 80, "I8Item layout");
 
-struct I8Unit {
-  int item0, n_items;  // items [item0, item0 + n_items), one batch
-  int batch, nc, ib_off, t;
-  int n_nt, n_kc;  // N tiles of 32 rows, K chunks of 32
+// One N tile of one batch and perturbation, packed by one CTA.
+struct I8BTile {
+  int ib_off, nc, jn, t;
+  int n_rows, n_kc, sb_off, pad_;  // rows of this tile (32; rows past n_compute are zero)
+  long long b_off;                 // bytes of the tile's first chunk
 };
-static_assert(sizeof(I8Unit) == 32, "I8Unit layout");
+static_assert(sizeof(I8BTile) == 40, "I8BTile layout");
 
 struct I8Group {
-  int item0, item1;  // items [item0, item1)
-  int unit0, unit1;  // units [unit0, unit1)
-  long long a_bytes;
-  int sa_len, pad_;
+  int item0, item1;   // items [item0, item1)
+  int tile0, tile1;   // B tiles [tile0, tile1)
+  long long a_bytes, b_bytes;
+  int sa_len, sb_len;
 };
 
 struct Rho1Plan {
@@ -186,15 +191,19 @@ struct Rho1Plan {
   int order = 0;               // 0: largest items first, 1: batch order
   std::vector<Rho1WorkItem> h_batches;
   std::vector<int> h_ib;  // host copy of the compact basis lists
-  // split-int8 path: work lists (built with the plan) and the packed-phi
-  // scratch (allocated by the first split-int8 execution, reused afterwards)
+  // split-int8 path: work lists (built with the plan) and the scratch
+  // (allocated by the first split-int8 execution, reused afterwards)
   I8Item *d_i8_items = nullptr;
-  I8Unit *d_i8_units = nullptr;
+  I8BTile *d_i8_tiles = nullptr;
   std::vector<I8Group> i8_groups;
-  long long i8_budget = 4LL << 30;  // bytes of A scratch per group
+  long long i8_budget = 4LL << 30;  // bytes of A + B scratch per group
   int i8_wave4 = 0;                  // every batch's phi offset a multiple of 4 doubles
-  unsigned char *d_i8_a = nullptr;
-  double *d_i8_sa = nullptr;
+  // two scratch sets: group g is packed into set g % 2 on a side stream while
+  // group g - 1 is contracted on the caller's stream
+  unsigned char *d_i8_a[2] = {nullptr, nullptr}, *d_i8_b[2] = {nullptr, nullptr};
+  double *d_i8_sa[2] = {nullptr, nullptr}, *d_i8_sb[2] = {nullptr, nullptr};
+  cudaStream_t i8_side = nullptr;
+  cudaEvent_t i8_ev_start = nullptr, i8_ev_packed[2] = {nullptr, nullptr}, i8_ev_done[2] = {nullptr, nullptr};
 };
 
 // Work lists of a plan's valid batches (one entry per batch in `batches`).

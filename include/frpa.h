@@ -62,8 +62,7 @@ int frpa_get_atom_tile_size(void);
  *   FRPA_RHO1_FP64        FP64 tensor-core tiles (DMMA), the reference's arithmetic;
  *   FRPA_RHO1_SPLIT_BF16  five BF16 slices per operand on tcgen05 kind::f16, FP32 level sums;
  *   FRPA_RHO1_SPLIT_I8    five signed 8-bit digits per operand on tcgen05 kind::i8, exact
- *                         int32 level sums; phi packed by a separate kernel, P1c built
- *                         in shared memory by the contraction. */
+ *                         int32 level sums, operands packed by separate kernels. */
 enum { FRPA_RHO1_FP64 = 0, FRPA_RHO1_SPLIT_BF16 = 1, FRPA_RHO1_SPLIT_I8 = 2 };
 int frpa_set_rho1_mode(int mode);
 int frpa_get_rho1_mode(void);
@@ -277,9 +276,9 @@ int frpa_rho1_plan_create(frpa_rho1_plan **plan, const frpa_rho1_desc *desc);
 int frpa_rho1_plan_destroy(frpa_rho1_plan *plan);
 /* Work-list statistics: [n_items, n_valid_batches, n_valid_points]. */
 int frpa_rho1_plan_info(const frpa_rho1_plan *plan, long long *info3);
-/* Split-int8 mode: [groups, point tiles, contraction units, largest packed-phi
- * scratch of a group in bytes] (no counterpart in the reference).  Each group
- * is two kernel launches (pack phi, contraction with P1c built on chip). */
+/* Split-int8 mode: [groups, work items, packed P1c tiles, largest A + B scratch
+ * of a group in bytes] (no counterpart in the reference).  Each group is three
+ * kernel launches (pack phi, pack P1c, contraction). */
 int frpa_rho1_plan_i8_info(const frpa_rho1_plan *plan, long long *info4);
 
 /* rho1 and grad rho1 for perturbations t < T; rho1 is written for
