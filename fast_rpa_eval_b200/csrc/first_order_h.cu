@@ -258,7 +258,7 @@ __device__ __forceinline__ void add_fixed(unsigned long long *lo, unsigned long 
 // ----------------------------------------------------------------- tiles
 
 template <bool SYM>
-__global__ void __launch_bounds__(THREADS) h1_tile_kernel(const H1Item *__restrict__ items, int n_items, H1Args a) {
+__global__ void __launch_bounds__(THREADS, 2) h1_tile_kernel(const H1Item *__restrict__ items, int n_items, H1Args a) {
   __shared__ __align__(16) double As[KC * LDA];  // A(m0 + m, k)
   __shared__ __align__(16) double Bs[BN * LDB];  // phi(n0 + n, k)
   __shared__ __align__(16) double Ps[SYM ? KC * LDA : 1];  // phi(m0 + m, k)
@@ -290,36 +290,38 @@ __global__ void __launch_bounds__(THREADS) h1_tile_kernel(const H1Item *__restri
     for (int k0 = 0; k0 < np; k0 += KC) {
       if (tid < KC && k0 + tid < np) coef[tid] = point_coef(a, W.batch, k0 + tid, W.prefix, t);
       __syncthreads();
+      {
+        // thread -> one point k of the chunk and four consecutive rows: the
+        // point's coefficients are read once, the rows' loads coalesce
+        constexpr int RPT = (BM * KC) / THREADS;  // rows per thread (4)
+        const int k = tid / (BM / RPT), r0 = (tid % (BM / RPT)) * RPT, p = k0 + k;
+        const bool pok = p < np;
+        const long long pc = (long long)(pok ? p : 0) * ncp;
+        const PointCoef c = coef[k];
+        const int jc = a.mode == 1 ? a.h.j_coord : 1;
+        const double *ph = phi + pc, *gp = gph + 3 * pc, *hp = hph ? hph + 6 * pc : nullptr;
 #pragma unroll
-      for (int j = 0; j < (BM * KC) / THREADS; ++j) {
-        const int e = tid + THREADS * j;
-        const int m = e & (BM - 1), k = e / BM;
-        const int i = W.m0 + m, p = k0 + k;
-        double va = 0.0, vp = 0.0;
-        if (i < nc && p < np) {
-          const long long pc = (long long)p * ncp;
-          va = a_value(coef[k], phi + pc, gph + 3 * pc, hph ? hph + 6 * pc : nullptr, i, ncp,
-                       hph != nullptr && i >= vs && i < ve, a.mode == 1 ? a.h.j_coord : 1);
-          if (SYM) vp = phi[i + pc];
+        for (int rr = 0; rr < RPT; ++rr) {
+          const int i = W.m0 + r0 + rr;
+          double va = 0.0, vp = 0.0;
+          if (pok && i < nc) {
+            va = a_value(c, ph, gp, hp, i, ncp, hp != nullptr && i >= vs && i < ve, jc);
+            if (SYM) vp = ph[i];
+          }
+          As[k * LDA + r0 + rr] = va;
+          if (SYM) Ps[k * LDA + r0 + rr] = vp;
         }
-        As[k * LDA + m] = va;
-        if (SYM) Ps[k * LDA + m] = vp;
-      }
 #pragma unroll
-      for (int j = 0; j < (BN * KC) / THREADS; ++j) {
-        const int e = tid + THREADS * j;
-        const int n = e & (BN - 1), k = e / BN;
-        const int jj = W.n0 + n, p = k0 + k;
-        double vb = 0.0, vq = 0.0;
-        if (jj < nc && p < np) {
-          const long long pc = (long long)p * ncp;
-          vb = phi[jj + pc];
-          if (SYM)
-            vq = a_value(coef[k], phi + pc, gph + 3 * pc, hph ? hph + 6 * pc : nullptr, jj, ncp,
-                         hph != nullptr && jj >= vs && jj < ve, a.mode == 1 ? a.h.j_coord : 1);
+        for (int rr = 0; rr < RPT; ++rr) {
+          const int jj = W.n0 + r0 + rr;
+          double vb = 0.0, vq = 0.0;
+          if (pok && jj < nc) {
+            vb = ph[jj];
+            if (SYM) vq = a_value(c, ph, gp, hp, jj, ncp, hp != nullptr && jj >= vs && jj < ve, jc);
+          }
+          Bs[(r0 + rr) * LDB + k] = vb;
+          if (SYM) Qs[(r0 + rr) * LDB + k] = vq;
         }
-        Bs[n * LDB + k] = vb;
-        if (SYM) Qs[n * LDB + k] = vq;
       }
       __syncthreads();
 #pragma unroll
