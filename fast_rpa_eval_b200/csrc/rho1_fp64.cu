@@ -23,8 +23,9 @@
 // task1_atom_tiling/version3_rho_with_bias/evaluate_first_order_rho.cu.hpp:93-254):
 // for perturbation t = atom j_atom_begin + t with compute range R,
 //   bias(p) = sum_i phi_i(p) sum_{k in R} (D(ib_i, ib_k) + D(ib_k, ib_i)) (-d phi_k / d x_jcoord)(p),
-// as extra K chunks after each row tile's main chunks (A: the two gathers of
-// D, B: the gradient of phi along j_coord), added to rho1 only.
+// as extra K chunks after each row tile's main chunks (A: the symmetrised
+// gather D(ib_i, ib_k) + D(ib_k, ib_i), B: the gradient of phi along j_coord),
+// added to rho1 only.
 #include <algorithm>
 #include <vector>
 
@@ -60,7 +61,7 @@ struct Smem {
   double red[2][4][BN];
   int ib[MAX_NC];
   int rs[FRPA_MAX_ATOM_TILE], re[FRPA_MAX_ATOM_TILE];  // fused bias: each perturbation's compute range
-  int nkb;                                             // fused bias: K chunks per row tile (both gathers)
+  int nkb;                                             // fused bias: K chunks per row tile
   int next;
 };
 
@@ -114,7 +115,7 @@ __global__ void __launch_bounds__(Fp64Shape<BN, BIAS>::THREADS, Fp64Shape<BN, BI
         S.re[t] = r1;
         rmax = max(rmax, r1 - r0);
       }
-      S.nkb = 2 * ((rmax + KC - 1) / KC);
+      S.nkb = (rmax + KC - 1) / KC;
     }
     __syncthreads();
 
@@ -134,20 +135,21 @@ __global__ void __launch_bounds__(Fp64Shape<BN, BIAS>::THREADS, Fp64Shape<BN, BI
       double *As = S.A[s % STAGES];
       double *Bs = S.B[s % STAGES];
       if (BIAS && kk >= nKc) {
-        // bias chunk: first the gather D(ib_i, ib_k), then D(ib_k, ib_i), over
-        // k in the perturbation's range; B = d phi_k / d x_jcoord
-        const int b = kk - nKc, hb = nKb / 2, tr = b / hb;
-        const int k0 = S.rs[t] + (b % hb) * KC, kend = S.re[t];
+        // bias chunk over k in the perturbation's range: A = D(ib_i, ib_k) +
+        // D(ib_k, ib_i), gathered with plain loads (the sum is formed on the
+        // way into shared memory); B = d phi_k / d x_jcoord
+        const int k0 = S.rs[t] + (kk - nKc) * KC, kend = S.re[t];
 #pragma unroll
         for (int j = 0; j < (BM * KC) / THREADS; ++j) {
           const int e = tid + THREADS * j;
           const int m = e & (BM - 1), k = e / BM;
           const int gm = m0 + m, gk = k0 + k;
-          const bool ok = gm < nc && gk < kend;
-          const double *src =
-              ok ? fb.dm + (tr == 0 ? S.ib[gm] + (long long)S.ib[gk] * n_basis : S.ib[gk] + (long long)S.ib[gm] * n_basis)
-                 : fb.dm;
-          cp_async_8(&As[k * LDA + m], src, ok ? 8 : 0);
+          double d = 0.0;
+          if (gm < nc && gk < kend) {
+            const long long bi = S.ib[gm], bk = S.ib[gk];
+            d = __ldg(fb.dm + bi + bk * n_basis) + __ldg(fb.dm + bk + bi * n_basis);
+          }
+          As[k * LDA + m] = d;
         }
 #pragma unroll
         for (int j = 0; j < (BN * KC) / THREADS; ++j) {
@@ -271,14 +273,16 @@ __global__ void __launch_bounds__(Fp64Shape<BN, BIAS>::THREADS, Fp64Shape<BN, BI
       const int mt = rest % nMt;
       const int t = rest / nMt;
       const int kc = kk;
-      const int k0 = (!BIAS || kk < nKc) ? kc * KC : 0, m0 = mt * BM;
+      const int k0 = kc * KC, m0 = mt * BM;
+      // valid K extent of this chunk: the compute functions, or the bias range
+      const int klim = (!BIAS || kk < nKc) ? nc - k0 : (S.re[t] - S.rs[t]) - (kk - nKc) * KC;
       const double *As = S.A[s % STAGES];
       const double *Bs = S.B[s % STAGES];
       const int row_w = m0 + wm * 32;
       const int col_w = wn * 16;
 #pragma unroll
       for (int ks = 0; ks < KC / 4; ++ks) {
-        if (k0 + ks * 4 < nc) {
+        if (ks * 4 < klim) {
           double a[4], b[2];
 #pragma unroll
           for (int mi = 0; mi < 4; ++mi) a[mi] = As[(ks * 4 + q) * LDA + wm * 32 + mi * 8 + g];
