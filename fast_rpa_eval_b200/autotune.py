@@ -21,11 +21,11 @@ import numpy as np
 from . import _lib
 
 FP64_SPACE = [
+    {"fp64_tile_points": 64, "fp64_ctas_per_sm": 0, "order": 2},
     {"fp64_tile_points": 64, "fp64_ctas_per_sm": 0, "order": 0},
-    {"fp64_tile_points": 64, "fp64_ctas_per_sm": 2, "order": 0},
+    {"fp64_tile_points": 64, "fp64_ctas_per_sm": 1, "order": 2},
     {"fp64_tile_points": 64, "fp64_ctas_per_sm": 0, "order": 1},
-    {"fp64_tile_points": 128, "fp64_ctas_per_sm": 0, "order": 0},
-    {"fp64_tile_points": 128, "fp64_ctas_per_sm": 0, "order": 1},
+    {"fp64_tile_points": 128, "fp64_ctas_per_sm": 0, "order": 2},
 ]
 # (the work order is shared by both paths' lists; the FP64 search owns it)
 SPLIT_SPACE = [

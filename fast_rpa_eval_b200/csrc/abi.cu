@@ -123,15 +123,16 @@ static int rho1_plan_build(Rho1Plan **out, const frpa_rho1_desc *D) {
     nc_max = std::max(nc_max, nc);
     ++n_valid_b;
     n_valid_pts += np;
-    batches.push_back(Rho1WorkItem{b, nc, np, 0, np, ib_off[b], pre, 0, off});
+    batches.push_back(Rho1WorkItem{b, nc, np, 0, np, ib_off[b], pre, rho1_locality_key(col, nc), off});
   }
   for (long long i = 0; i < map_len; ++i)
     FRPA_CHECK_ARG(D->i_valid_point_2_i_full_points_map[i] >= 0 &&
                        D->i_valid_point_2_i_full_points_map[i] < D->n_full_points,
                    "rho1: i_valid_point_2_i_full_points_map[%lld] = %d outside 0..%d", i,
                    D->i_valid_point_2_i_full_points_map[i], D->n_full_points - 1);
-  // largest first: the persistent kernel takes items in this order
-  rho1_fp64_build_items(batches, 64, 0, &items);
+  // locality order (batches sharing basis functions together, largest first
+  // within a key): the persistent kernel takes items in this order
+  rho1_fp64_build_items(batches, 64, 2, &items);
 
   Rho1Plan *P = new Rho1Plan();
   FRPA_CUDA_TRY(cudaGetDevice(&P->device));
@@ -509,7 +510,7 @@ int frpa_rho1_plan_set_tuning(frpa_rho1_plan *plan, int key, int value) {
       P.split_tile_points = value;
       break;
     case FRPA_TUNE_ORDER:
-      FRPA_CHECK_ARG(value == 0 || value == 1, "rho1 tuning: order %d not 0 or 1", value);
+      FRPA_CHECK_ARG(value >= 0 && value <= 2, "rho1 tuning: order %d not 0, 1 or 2", value);
       P.order = value;
       break;
     case FRPA_TUNE_SPLIT_I8_SCRATCH_MB:

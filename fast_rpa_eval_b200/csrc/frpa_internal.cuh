@@ -112,7 +112,7 @@ struct Rho1WorkItem {
   int pn;            // points in this tile
   int ib_off;        // offset of the batch's basis list in the compact list
   int prefix;        // n_point_batches_prefix_sum[batch]
-  int pad_;
+  int key;           // locality key: MinHash of the batch's basis functions
   long long wave_off;  // i_batch_2_wave_offset[batch]
 };
 static_assert(sizeof(Rho1WorkItem) == 40, "work item layout");
@@ -188,7 +188,7 @@ struct Rho1Plan {
   int fp64_tile_points = 64;   // 64 or 128 points per FP64 work item
   int fp64_ctas_per_sm = 0;    // 0: as many as fit
   int split_tile_points = 128; // <= 128 points per split-BF16 work item
-  int order = 0;               // 0: largest items first, 1: batch order
+  int order = 2;               // 0: largest items first, 1: batch order, 2: locality key
   std::vector<Rho1WorkItem> h_batches;
   std::vector<int> h_ib;  // host copy of the compact basis lists
   // split-int8 path: work lists (built with the plan) and the scratch
@@ -207,6 +207,9 @@ struct Rho1Plan {
 };
 
 // Work lists of a plan's valid batches (one entry per batch in `batches`).
+// work-list order (0 largest first, 1 batch order, 2 locality key) and the key
+void rho1_order_items(std::vector<Rho1WorkItem> *items, int order);
+int rho1_locality_key(const int *ib, int nc);
 void rho1_fp64_build_items(const std::vector<Rho1WorkItem> &batches, int tile_points, int order,
                            std::vector<Rho1WorkItem> *out);
 

@@ -35,30 +35,33 @@ namespace frpa {
 namespace {
 
 constexpr int BM = 64;       // rows (i_compute) per tile
-constexpr int KC = 16;       // contraction chunk
+constexpr int KC = 32;       // contraction chunk
 constexpr int STAGES = 2;    // cp.async pipeline depth (double buffering)
 constexpr int LDA = BM + 4;  // As[k][m]: stride = 4 (mod 16) doubles -> conflict-free fragment loads
-constexpr int LDB = KC + 4;  // Bs[n][k]
+constexpr int LDB = KC + 4;  // Bs[n][k]: stride = 4 (mod 16) doubles, rows 16-byte aligned
 constexpr int MAX_NC = FRPA_MAX_N_COMPUTE;
+constexpr int WM = BM / 32;  // warps along M (warp tile 32 x 16)
 
 // Tile shapes: BN points per work item, 2 warps along M x BN / 16 along N,
-// warp tile 32 x 16.  BN = 64: 256 threads, 3 CTAs per SM (80 registers,
-// 50 KB of shared memory each; measured faster than 2 CTAs with deeper
-// rings); BN = 128: 512 threads, one CTA per SM, each gathered P1c tile
-// serving twice the points.
+// warp tile 32 x 16, 32-wide K chunks.  BN = 64: 256 threads, 2 CTAs per SM
+// (84 KB of shared memory each, up to 128 registers); BN = 128: 512 threads,
+// one CTA per SM, each gathered P1c tile serving twice the points.
+// The loop is issue-bound, not MMA-bound, when its bookkeeping is heavy: every
+// step advances its (t, row tile, K chunk) position by increments (no integer
+// division), and warps whose 32 x 16 tile and K chunk are complete run an
+// unpredicated MMA loop.
 template <int BN, bool BIAS>
 struct Fp64Shape {
   static constexpr int WN = BN / 16;
-  static constexpr int THREADS = 64 * WN;
-  // the fused-bias form carries more state: two CTAs per SM instead of three
-  static constexpr int MIN_BLOCKS = BN == 64 ? (BIAS ? 2 : 3) : 1;
+  static constexpr int THREADS = 32 * WM * WN;
+  static constexpr int MIN_BLOCKS = (BN == 64 && BM == 64) ? 2 : 1;
 };
 
 template <int BN>
 struct Smem {
   double A[STAGES][KC * LDA];
   double B[STAGES][BN * LDB];
-  double red[2][4][BN];
+  double red[WM][4][BN];
   int ib[MAX_NC];
   int rs[FRPA_MAX_ATOM_TILE], re[FRPA_MAX_ATOM_TILE];  // fused bias: each perturbation's compute range
   int nkb;                                             // fused bias: K chunks per row tile
@@ -72,6 +75,17 @@ struct FusedBias {
   int n_atoms, j_atom_begin, j_coord;
   int *err;               // device flags: bit 3 = a range leaves its batch (clipped)
 };
+
+// (K chunk, row tile, t) of one step, advanced by one step
+__device__ __forceinline__ void step_advance(int &kk, int &mt, int &t, int nKs, int nMt) {
+  if (++kk == nKs) {
+    kk = 0;
+    if (++mt == nMt) {
+      mt = 0;
+      ++t;
+    }
+  }
+}
 
 template <int BN, bool BIAS>
 __global__ void __launch_bounds__(Fp64Shape<BN, BIAS>::THREADS, Fp64Shape<BN, BIAS>::MIN_BLOCKS)
@@ -126,14 +140,14 @@ __global__ void __launch_bounds__(Fp64Shape<BN, BIAS>::THREADS, Fp64Shape<BN, BI
     const int nKb = BIAS ? S.nkb : 0, nKs = nKc + nKb;  // K chunks per (t, row tile): main, then the bias's
     const int steps = T * nMt * nKs;
 
-    auto load = [&](int s) {
-      const int kk = s % nKs;
-      const int rest = s / nKs;
-      const int mt = rest % nMt;
-      const int t = rest / nMt;
+    // position of the next chunk to load (runs STAGES - 1 steps ahead)
+    int ld_kk = 0, ld_mt = 0, ld_t = 0;
+    auto load = [&](int stage) {
+      const int kk = ld_kk, mt = ld_mt, t = ld_t;
+      step_advance(ld_kk, ld_mt, ld_t, nKs, nMt);
       const int m0 = mt * BM;
-      double *As = S.A[s % STAGES];
-      double *Bs = S.B[s % STAGES];
+      double *As = S.A[stage];
+      double *Bs = S.B[stage];
       if (BIAS && kk >= nKc) {
         // bias chunk over k in the perturbation's range: A = D(ib_i, ib_k) +
         // D(ib_k, ib_i), gathered with plain loads (the sum is formed on the
@@ -162,17 +176,19 @@ __global__ void __launch_bounds__(Fp64Shape<BN, BIAS>::THREADS, Fp64Shape<BN, BI
         }
         return;
       }
-      const int kc = kk;
-      const int k0 = kc * KC;
+      const int k0 = kk * KC;
       const double *P = P1 + t * nb2;
+      // A: this thread's row is fixed (THREADS is a multiple of BM); its
+      // columns step by THREADS / BM
+      const int m = tid & (BM - 1), gm = m0 + m;
+      const bool row_ok = gm < nc;
+      const double *Prow = P + (row_ok ? S.ib[gm] : 0);
 #pragma unroll
       for (int j = 0; j < (BM * KC) / THREADS; ++j) {
-        const int e = tid + THREADS * j;
-        const int m = e & (BM - 1), k = e / BM;
-        const int gm = m0 + m, gk = k0 + k;
-        const bool ok = gm < nc && gk < nc;
-        const double *src = ok ? P + S.ib[gm] + (long long)S.ib[gk] * n_basis : P;
-        cp_async_8(&As[k * LDA + m], src, ok ? 8 : 0);
+        const int k = tid / BM + (THREADS / BM) * j;
+        const int gk = k0 + k;
+        const bool ok = row_ok && gk < nc;
+        cp_async_8(&As[k * LDA + m], ok ? Prow + (long long)S.ib[gk] * n_basis : P, ok ? 8 : 0);
       }
       if (aligned16) {
 #pragma unroll
@@ -244,10 +260,14 @@ __global__ void __launch_bounds__(Fp64Shape<BN, BIAS>::THREADS, Fp64Shape<BN, BI
       __syncthreads();
       if (tid < pn) {
         const int p = W.p0 + tid;
-        const double r = S.red[0][0][tid] + S.red[1][0][tid];
-        const double gx = S.red[0][1][tid] + S.red[1][1][tid];
-        const double gy = S.red[0][2][tid] + S.red[1][2][tid];
-        const double gz = S.red[0][3][tid] + S.red[1][3][tid];
+        double r = S.red[0][0][tid], gx = S.red[0][1][tid], gy = S.red[0][2][tid], gz = S.red[0][3][tid];
+#pragma unroll
+        for (int w = 1; w < WM; ++w) {
+          r += S.red[w][0][tid];
+          gx += S.red[w][1][tid];
+          gy += S.red[w][2][tid];
+          gz += S.red[w][3][tid];
+        }
         const long long bidx = p + (long long)n_max_batch_size * (W.batch + (long long)n_batches * t);
         const long long gi = 3 * bidx;
         grad[gi + 0] = gx * 2 - gbias[gi + 0];
@@ -262,27 +282,24 @@ __global__ void __launch_bounds__(Fp64Shape<BN, BIAS>::THREADS, Fp64Shape<BN, BI
       __syncthreads();
     };
 
+    const int col_w = wn * 16;
+    int kk = 0, mt = 0, t = 0;
     for (int s = 0; s < steps; ++s) {
       cp_async_wait<STAGES - 2>();
       __syncthreads();
-      if (s + STAGES - 1 < steps) load(s + STAGES - 1);
+      if (s + STAGES - 1 < steps) load((s + STAGES - 1) % STAGES);
       cp_async_commit();
 
-      const int kk = s % nKs;
-      const int rest = s / nKs;
-      const int mt = rest % nMt;
-      const int t = rest / nMt;
-      const int kc = kk;
-      const int k0 = kc * KC, m0 = mt * BM;
-      // valid K extent of this chunk: the compute functions, or the bias range
-      const int klim = (!BIAS || kk < nKc) ? nc - k0 : (S.re[t] - S.rs[t]) - (kk - nKc) * KC;
+      const int m0 = mt * BM;
       const double *As = S.A[s % STAGES];
       const double *Bs = S.B[s % STAGES];
       const int row_w = m0 + wm * 32;
-      const int col_w = wn * 16;
+      // valid K extent of this chunk: the compute functions, or the bias range
+      const int klim = (!BIAS || kk < nKc) ? nc - kk * KC : (S.re[t] - S.rs[t]) - (kk - nKc) * KC;
+      if (row_w + 32 <= nc && col_w + 16 <= pn && klim >= KC) {
+        // complete warp tile and chunk: no predicates
 #pragma unroll
-      for (int ks = 0; ks < KC / 4; ++ks) {
-        if (ks * 4 < klim) {
+        for (int ks = 0; ks < KC / 4; ++ks) {
           double a[4], b[2];
 #pragma unroll
           for (int mi = 0; mi < 4; ++mi) a[mi] = As[(ks * 4 + q) * LDA + wm * 32 + mi * 8 + g];
@@ -291,12 +308,28 @@ __global__ void __launch_bounds__(Fp64Shape<BN, BIAS>::THREADS, Fp64Shape<BN, BI
 #pragma unroll
           for (int mi = 0; mi < 4; ++mi)
 #pragma unroll
-            for (int ni = 0; ni < 2; ++ni)
-              if (row_w + mi * 8 < nc && col_w + ni * 8 < pn) dmma_8x8x4(acc[mi][ni][0], acc[mi][ni][1], a[mi], b[ni]);
+            for (int ni = 0; ni < 2; ++ni) dmma_8x8x4(acc[mi][ni][0], acc[mi][ni][1], a[mi], b[ni]);
+        }
+      } else if (row_w < nc && col_w < pn) {
+        const int nmi = min(4, (nc - row_w + 7) / 8), nni = min(2, (pn - col_w + 7) / 8);
+#pragma unroll
+        for (int ks = 0; ks < KC / 4; ++ks) {
+          if (ks * 4 < klim) {
+            double a[4], b[2];
+#pragma unroll
+            for (int mi = 0; mi < 4; ++mi) a[mi] = As[(ks * 4 + q) * LDA + wm * 32 + mi * 8 + g];
+#pragma unroll
+            for (int ni = 0; ni < 2; ++ni) b[ni] = Bs[(col_w + ni * 8 + g) * LDB + ks * 4 + q];
+#pragma unroll
+            for (int mi = 0; mi < 4; ++mi)
+#pragma unroll
+              for (int ni = 0; ni < 2; ++ni)
+                if (mi < nmi && ni < nni) dmma_8x8x4(acc[mi][ni][0], acc[mi][ni][1], a[mi], b[ni]);
+          }
         }
       }
 
-      if (kc == nKc - 1) {
+      if (kk == nKc - 1) {
         // epilogue of one work1 tile: contract with phi and grad phi
 #pragma unroll
         for (int mi = 0; mi < 4; ++mi) {
@@ -339,6 +372,7 @@ __global__ void __launch_bounds__(Fp64Shape<BN, BIAS>::THREADS, Fp64Shape<BN, BI
         }
       }
       if (BIAS && kk == nKs - 1 && mt == nMt - 1) finish(t);
+      step_advance(kk, mt, t, nKs, nMt);
     }
     cp_async_wait<0>();
     __syncthreads();
@@ -425,8 +459,40 @@ int rho1_fp64_fused_bias_launch(const Rho1Plan &plan, int n_active, int n_atoms,
   return fp64_run(plan, n_active, wave, gwave, P1, bias, gbias, rho, grad, &fb, stream);
 }
 
+// Orders a work list: 0 largest nc^2 x points first, 1 batch order, 2 by the
+// batches' locality key (batches sharing basis functions run together, so
+// the density-matrix blocks they gather stay in L2), largest first within a key.
+void rho1_order_items(std::vector<Rho1WorkItem> *items, int order) {
+  auto cost = [](const Rho1WorkItem &a) { return (long long)a.nc * a.nc * a.pn; };
+  if (order == 0)
+    std::stable_sort(items->begin(), items->end(),
+                     [&](const Rho1WorkItem &a, const Rho1WorkItem &b) { return cost(a) > cost(b); });
+  else if (order == 2)
+    std::stable_sort(items->begin(), items->end(), [&](const Rho1WorkItem &a, const Rho1WorkItem &b) {
+      if (a.key != b.key) return (unsigned)a.key < (unsigned)b.key;
+      return cost(a) > cost(b);
+    });
+}
+
+// MinHash of a batch's basis list (1-based indices): the smallest 32-bit
+// integer hash over its functions (Wellons' lowbias32 mixer).  Batches whose
+// lists overlap a lot share it with high probability.
+int rho1_locality_key(const int *ib, int nc) {
+  unsigned best = 0xffffffffu;
+  for (int i = 0; i < nc; ++i) {
+    unsigned x = (unsigned)ib[i];
+    x ^= x >> 16;
+    x *= 0x7feb352du;
+    x ^= x >> 15;
+    x *= 0x846ca68bu;
+    x ^= x >> 16;
+    best = std::min(best, x);
+  }
+  return (int)best;
+}
+
 // Work items of <= tile_points points (a batch's points split evenly, widths a
-// multiple of 8), largest nc^2 x points first or in batch order.
+// multiple of 8), in the given order.
 void rho1_fp64_build_items(const std::vector<Rho1WorkItem> &batches, int tile_points, int order,
                            std::vector<Rho1WorkItem> *out) {
   out->clear();
@@ -436,13 +502,10 @@ void rho1_fp64_build_items(const std::vector<Rho1WorkItem> &batches, int tile_po
     int w = (b.np + tiles - 1) / tiles;
     w = std::min(tile_points, (w + 7) & ~7);
     for (int p0 = 0; p0 < b.np; p0 += w)
-      out->push_back(Rho1WorkItem{b.batch, b.nc, b.np, p0, std::min(w, b.np - p0), b.ib_off, b.prefix, 0,
+      out->push_back(Rho1WorkItem{b.batch, b.nc, b.np, p0, std::min(w, b.np - p0), b.ib_off, b.prefix, b.key,
                                   b.wave_off});
   }
-  if (order == 0)
-    std::stable_sort(out->begin(), out->end(), [](const Rho1WorkItem &a, const Rho1WorkItem &b) {
-      return (long long)a.nc * a.nc * a.pn > (long long)b.nc * b.nc * b.pn;
-    });
+  rho1_order_items(out, order);
 }
 
 }  // namespace frpa

@@ -651,13 +651,10 @@ void rho1_split_build_items(const std::vector<Rho1WorkItem> &batches, int tile_p
     const int tiles = (np + tp - 1) / tp;
     const int width = (np + tiles - 1) / tiles;
     for (int p0 = 0; p0 < np; p0 += width)
-      out->push_back(Rho1WorkItem{w.batch, w.nc, w.np, p0, std::min(width, np - p0), w.ib_off, w.prefix, 0,
+      out->push_back(Rho1WorkItem{w.batch, w.nc, w.np, p0, std::min(width, np - p0), w.ib_off, w.prefix, w.key,
                                   w.wave_off});
   }
-  if (order == 0)
-    std::stable_sort(out->begin(), out->end(), [](const Rho1WorkItem &a, const Rho1WorkItem &b) {
-      return (long long)a.nc * a.nc * a.pn > (long long)b.nc * b.nc * b.pn;
-    });
+  rho1_order_items(out, order);
 }
 
 }  // namespace frpa

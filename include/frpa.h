@@ -318,12 +318,15 @@ int frpa_rho1_bias_part2(const frpa_rho1_plan *plan, int T, int n_atoms, int j_a
 
 /* Tunings of a plan's rho1 launches (no counterpart in the reference, whose
  * MAGMA batching has fixed shapes).  Keys and values:
- *   FRPA_TUNE_FP64_TILE_POINTS  64 (256 threads, up to 3 CTAs per SM) or 128
+ *   FRPA_TUNE_FP64_TILE_POINTS  64 (256 threads, up to 2 CTAs per SM) or 128
  *                               (512 threads, 1 CTA per SM: each gathered P1c
  *                               tile serves twice the points);
  *   FRPA_TUNE_FP64_CTAS_PER_SM  0 (as many as fit), 1, 2 or 3;
  *   FRPA_TUNE_SPLIT_TILE_POINTS 16..128 points per split-BF16 work item;
- *   FRPA_TUNE_ORDER             0 largest items first, 1 batch order;
+ *   FRPA_TUNE_ORDER             0 largest items first, 1 batch order, 2 (the
+ *                               default) batches grouped by a MinHash of their
+ *                               basis lists, so batches sharing functions run
+ *                               together and their P1 blocks stay in L2;
  *   FRPA_TUNE_SPLIT_I8_SCRATCH_MB  MiB of packed-operand scratch per group of
  *                               batches in the split-int8 mode (default 4096;
  *                               the batches are packed and contracted group by

@@ -71,7 +71,7 @@ def test_every_tuning_gives_identical_results(mode):
 def test_tuning_rejects_bad_values():
     p, _ = _setup()
     plan = _lib.Rho1Plan(p)
-    for kw in ({"fp64_tile_points": 96}, {"fp64_ctas_per_sm": 4}, {"split_tile_points": 200}, {"order": 2}):
+    for kw in ({"fp64_tile_points": 96}, {"fp64_ctas_per_sm": 4}, {"split_tile_points": 200}, {"order": 3}):
         with pytest.raises(_lib.FrpaError):
             plan.set_tuning(**kw)
 
