@@ -46,7 +46,8 @@
 namespace frpa {
 
 constexpr int SU_LMAX = FRPA_SUMUP_MAX_L;  // 8
-constexpr int SU_THREADS = 128;
+constexpr int SU_THREADS = 128;  // fast kernel: 5 CTAs per SM, 96 registers (no spills; measured against
+                                 // 3, 4 and 6 CTAs per SM and two centres per thread)
 constexpr int SU_PPT = 2;                  // points per thread (share coefficient loads)
 constexpr int SU_CHUNK = 16;               // centre records staged per shared-memory chunk
 
@@ -240,7 +241,7 @@ __device__ double near_field(int lam, int L2, double dx, double dy, double dz, d
 
 // --------------------------------------------------------- fast kernel ---
 
-__global__ void __launch_bounds__(SU_THREADS)
+__global__ void __launch_bounds__(SU_THREADS, 5)
     sumup_fast_kernel(int n_valid, int n_full, const int *__restrict__ map, const int *__restrict__ order,
                       const double *__restrict__ coord, int n_active, int n_chp, int n_atoms, int L,
                       int n_hartree_grid, const double *__restrict__ recs, const double *__restrict__ spline,
