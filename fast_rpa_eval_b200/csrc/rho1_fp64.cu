@@ -14,8 +14,11 @@
 // shared memory, the contraction runs on the FP64 tensor-core MMA
 // (mma.sync m8n8k4 f64) with the accumulators in registers, and the epilogue
 // contracts each finished work1 tile against phi / grad phi, so work1 never
-// leaves the SM.  Per-point sums are reduced in a fixed order (registers ->
-// warp shuffles -> two shared-memory slots), so results are deterministic.
+// leaves the SM: the tile is staged in the shared-memory stage its last K
+// chunk used, and each warp then reads whole point rows of phi / grad phi
+// with 16-byte loads.  Per-point sums are reduced in a fixed order (lane
+// pairs -> recursive halving over the warp -> row tiles in order), so results
+// are deterministic.
 //
 // Optionally the same launch also computes the ground-state density-matrix
 // part of the rho1 bias (what generate_first_order_rho_bias_part2.cpp:84-150
@@ -41,6 +44,13 @@ constexpr int LDA = BM + 4;  // As[k][m]: stride = 4 (mod 16) doubles -> conflic
 constexpr int LDB = KC + 4;  // Bs[n][k]: stride = 4 (mod 16) doubles, rows 16-byte aligned
 constexpr int MAX_NC = FRPA_MAX_N_COMPUTE;
 constexpr int WM = BM / 32;  // warps along M (warp tile 32 x 16)
+// Epilogue staging: a finished 64-row work1 tile is written to the stage that
+// its last K chunk used (rows 0-31 in A's buffer, rows 32-63 in B's), 64
+// points per round, each point's 32 rows at a stride of LDW doubles
+// (LDW = 2 mod 8: the fragment stores are conflict-free, rows 16-byte aligned).
+constexpr int LDW = 34;
+static_assert(BM == 64, "the epilogue staging assumes 64-row tiles");
+static_assert(64 * LDW <= KC * LDA && 64 * LDW <= 64 * LDB, "a 64-point work1 half-tile fits a stage buffer");
 
 // Tile shapes: BN points per work item, 2 warps along M x BN / 16 along N,
 // warp tile 32 x 16, 32-wide K chunks.  BN = 64: 256 threads, 2 CTAs per SM
@@ -101,6 +111,7 @@ __global__ void __launch_bounds__(Fp64Shape<BN, BIAS>::THREADS, Fp64Shape<BN, BI
   const int tid = threadIdx.x;
   const int lane = tid & 31, warp = tid >> 5;
   const int wm = warp / WN, wn = warp % WN;
+  const int col_w = wn * 16;  // this warp's first point in the tile
   const int g = lane >> 2, q = lane & 3;
   const long long nb2 = (long long)n_basis * n_basis;
 
@@ -214,15 +225,18 @@ __global__ void __launch_bounds__(Fp64Shape<BN, BIAS>::THREADS, Fp64Shape<BN, BI
     };
 
     double acc[4][2][2];
-    double s_r[2][2], s_x[2][2], s_y[2][2], s_z[2][2];
 #pragma unroll
     for (int a = 0; a < 4; ++a)
 #pragma unroll
       for (int b = 0; b < 2; ++b) acc[a][b][0] = acc[a][b][1] = 0.0;
+    // per-point sums: after each row tile's epilogue lane l of warp w holds the
+    // sum (over rows so far) of component c = (l % NV) / PPW (rho1, d/dx, d/dy,
+    // d/dz) of point w PPW + (l % NV) % PPW of each 64-point round
+    constexpr int ROUNDS = BN / 64, NWARP = THREADS / 32, PPW = 64 / NWARP, NV = 4 * PPW;
+    static_assert(NV == 16 || NV == 32, "per-lane reduction shape");
+    double tot[ROUNDS];
 #pragma unroll
-    for (int b = 0; b < 2; ++b)
-#pragma unroll
-      for (int h = 0; h < 2; ++h) s_r[b][h] = s_x[b][h] = s_y[b][h] = s_z[b][h] = 0.0;
+    for (int r = 0; r < ROUNDS; ++r) tot[r] = 0.0;
 
 #pragma unroll
     for (int s = 0; s < STAGES - 1; ++s) {
@@ -230,44 +244,21 @@ __global__ void __launch_bounds__(Fp64Shape<BN, BIAS>::THREADS, Fp64Shape<BN, BI
       cp_async_commit();
     }
 
-    // all rows of perturbation t done: reduce the per-point sums over rows,
-    // write rho1 and grad rho1, clear the sums
+    // all rows of perturbation t done: gather the per-lane sums by point, write
+    // rho1 and grad rho1, clear the sums
     auto finish = [&](int t) {
+      if (lane < NV) {
 #pragma unroll
-      for (int ni = 0; ni < 2; ++ni)
-#pragma unroll
-        for (int h = 0; h < 2; ++h) {
-#pragma unroll
-          for (int off = 4; off < 32; off <<= 1) {
-            s_r[ni][h] += __shfl_xor_sync(0xffffffffu, s_r[ni][h], off);
-            s_x[ni][h] += __shfl_xor_sync(0xffffffffu, s_x[ni][h], off);
-            s_y[ni][h] += __shfl_xor_sync(0xffffffffu, s_y[ni][h], off);
-            s_z[ni][h] += __shfl_xor_sync(0xffffffffu, s_z[ni][h], off);
-          }
+        for (int r = 0; r < ROUNDS; ++r) {
+          const int idx = lane & (NV - 1);
+          S.red[0][idx / PPW][r * 64 + warp * PPW + idx % PPW] = tot[r];
+          tot[r] = 0.0;
         }
-      if (g == 0) {
-#pragma unroll
-        for (int ni = 0; ni < 2; ++ni)
-#pragma unroll
-          for (int h = 0; h < 2; ++h) {
-            const int col = wn * 16 + ni * 8 + 2 * q + h;
-            S.red[wm][0][col] = s_r[ni][h];
-            S.red[wm][1][col] = s_x[ni][h];
-            S.red[wm][2][col] = s_y[ni][h];
-            S.red[wm][3][col] = s_z[ni][h];
-          }
       }
       __syncthreads();
       if (tid < pn) {
         const int p = W.p0 + tid;
-        double r = S.red[0][0][tid], gx = S.red[0][1][tid], gy = S.red[0][2][tid], gz = S.red[0][3][tid];
-#pragma unroll
-        for (int w = 1; w < WM; ++w) {
-          r += S.red[w][0][tid];
-          gx += S.red[w][1][tid];
-          gy += S.red[w][2][tid];
-          gz += S.red[w][3][tid];
-        }
+        const double r = S.red[0][0][tid], gx = S.red[0][1][tid], gy = S.red[0][2][tid], gz = S.red[0][3][tid];
         const long long bidx = p + (long long)n_max_batch_size * (W.batch + (long long)n_batches * t);
         const long long gi = 3 * bidx;
         grad[gi + 0] = gx * 2 - gbias[gi + 0];
@@ -275,14 +266,86 @@ __global__ void __launch_bounds__(Fp64Shape<BN, BIAS>::THREADS, Fp64Shape<BN, BI
         grad[gi + 2] = gz * 2 - gbias[gi + 2];
         if (t < n_active) rho[map[W.prefix + p] + (long long)n_full_points * t] = r + bias[bidx];
       }
-#pragma unroll
-      for (int ni = 0; ni < 2; ++ni)
-#pragma unroll
-        for (int h = 0; h < 2; ++h) s_r[ni][h] = s_x[ni][h] = s_y[ni][h] = s_z[ni][h] = 0.0;
       __syncthreads();
     };
 
-    const int col_w = wn * 16;
+    // Epilogue of one finished tile (acc = work1 rows m0.., or the bias tile):
+    // acc goes to this step's stage buffers, then each warp contracts PPW
+    // points with phi (and grad phi): lane l takes rows 2l, 2l + 1 of a point
+    // (16-byte loads, 512 contiguous bytes per warp and array), and the NV
+    // per-lane products are summed over the 32 lanes by recursive halving
+    // (31 shuffles), lane l keeping value l % NV.  Main tiles add all four
+    // components; bias tiles subtract from rho1 only.
+    auto tile_epilogue = [&](int stage, int m0, bool bias_tile) {
+      double *Wa = S.A[stage], *Wb = S.B[stage];
+      __syncthreads();  // every warp's MMAs are done with this stage's operands
+#pragma unroll
+      for (int round = 0; round < ROUNDS; ++round) {
+        if (col_w / 64 == round) {
+          double *Wh = wm == 0 ? Wa : Wb;
+#pragma unroll
+          for (int mi = 0; mi < 4; ++mi)
+#pragma unroll
+            for (int ni = 0; ni < 2; ++ni)
+#pragma unroll
+              for (int h = 0; h < 2; ++h)
+                Wh[((col_w & 63) + ni * 8 + 2 * q + h) * LDW + mi * 8 + g] = acc[mi][ni][h];
+        }
+        __syncthreads();
+        double v[NV];
+        const int r0 = m0 + 2 * lane;
+        const bool in_block = r0 < ncp, ok0 = r0 < nc, ok1 = r0 + 1 < nc;
+#pragma unroll
+        for (int j = 0; j < PPW; ++j) {
+          const int pl = warp * PPW + j, p = round * 64 + pl;
+#pragma unroll
+          for (int c = 0; c < 4; ++c) v[c * PPW + j] = 0.0;
+          if (p < pn && in_block) {
+            const double2 w = *reinterpret_cast<const double2 *>((lane < 16 ? Wa : Wb) + pl * LDW + 2 * (lane & 15));
+#pragma unroll
+            for (int c = 0; c < 4; ++c) {
+              if (bias_tile && c > 0) continue;
+              const double *src =
+                  c == 0 ? phi + r0 + (long long)p * ncp : gph + r0 + (long long)ncp * (3LL * p + (c - 1));
+              double x0, x1;
+              if (aligned16) {
+                const double2 x = __ldg(reinterpret_cast<const double2 *>(src));
+                x0 = x.x;
+                x1 = x.y;
+              } else {
+                x0 = __ldg(src);
+                x1 = __ldg(src + 1);
+              }
+              v[c * PPW + j] = fma(ok1 ? x1 : 0.0, w.y, (ok0 ? x0 : 0.0) * w.x);
+            }
+          }
+        }
+        // sum over the 32 lanes: fold the offsets >= NV, then halve
+#pragma unroll
+        for (int o = 16; o >= NV; o >>= 1)
+#pragma unroll
+          for (int i = 0; i < NV; ++i) v[i] += __shfl_xor_sync(0xffffffffu, v[i], o);
+#pragma unroll
+        for (int o = NV / 2; o >= 1; o >>= 1) {
+          const bool upper = (lane & o) != 0;
+#pragma unroll
+          for (int i = 0; i < o; ++i) {
+            const double keep = upper ? v[i + o] : v[i], give = upper ? v[i] : v[i + o];
+            v[i] = keep + __shfl_xor_sync(0xffffffffu, give, o);
+          }
+        }
+        if (bias_tile)
+          tot[round] -= v[0];
+        else
+          tot[round] += v[0];
+        if (round + 1 < ROUNDS) __syncthreads();  // the next round rewrites the staging
+      }
+#pragma unroll
+      for (int mi = 0; mi < 4; ++mi)
+#pragma unroll
+        for (int ni = 0; ni < 2; ++ni) acc[mi][ni][0] = acc[mi][ni][1] = 0.0;
+    };
+
     int kk = 0, mt = 0, t = 0;
     for (int s = 0; s < steps; ++s) {
       cp_async_wait<STAGES - 2>();
@@ -330,47 +393,11 @@ __global__ void __launch_bounds__(Fp64Shape<BN, BIAS>::THREADS, Fp64Shape<BN, BI
       }
 
       if (kk == nKc - 1) {
-        // epilogue of one work1 tile: contract with phi and grad phi
-#pragma unroll
-        for (int mi = 0; mi < 4; ++mi) {
-          const int row = row_w + mi * 8 + g;
-          if (row < nc) {
-#pragma unroll
-            for (int ni = 0; ni < 2; ++ni)
-#pragma unroll
-              for (int h = 0; h < 2; ++h) {
-                const int col = col_w + ni * 8 + 2 * q + h;
-                if (col < pn) {
-                  const double w1 = acc[mi][ni][h];
-                  const long long pc = (long long)col * ncp;
-                  s_r[ni][h] += __ldg(phi + row + pc) * w1;
-                  const double *gp = gph + row + 3 * pc;
-                  s_x[ni][h] += __ldg(gp) * w1;
-                  s_y[ni][h] += __ldg(gp + ncp) * w1;
-                  s_z[ni][h] += __ldg(gp + 2 * ncp) * w1;
-                }
-              }
-          }
-#pragma unroll
-          for (int ni = 0; ni < 2; ++ni) acc[mi][ni][0] = acc[mi][ni][1] = 0.0;
-        }
+        tile_epilogue(s % STAGES, m0, false);  // work1 tile: contract with phi and grad phi
         if (!BIAS && mt == nMt - 1) finish(t);
       }
-      if (BIAS && nKb > 0 && kk == nKs - 1) {
-        // the bias of this row tile: rho1 -= sum_i phi_i (S d phi / d x_jcoord)_i
-#pragma unroll
-        for (int mi = 0; mi < 4; ++mi) {
-          const int row = row_w + mi * 8 + g;
-#pragma unroll
-          for (int ni = 0; ni < 2; ++ni)
-#pragma unroll
-            for (int h = 0; h < 2; ++h) {
-              const int col = col_w + ni * 8 + 2 * q + h;
-              if (row < nc && col < pn) s_r[ni][h] -= __ldg(phi + row + (long long)col * ncp) * acc[mi][ni][h];
-              acc[mi][ni][h] = 0.0;
-            }
-        }
-      }
+      // the bias of this row tile: rho1 -= sum_i phi_i (S d phi / d x_jcoord)_i
+      if (BIAS && nKb > 0 && kk == nKs - 1) tile_epilogue(s % STAGES, m0, true);
       if (BIAS && kk == nKs - 1 && mt == nMt - 1) finish(t);
       step_advance(kk, mt, t, nKs, nMt);
     }
