@@ -10,6 +10,7 @@
 #include <atomic>
 #include <cstdlib>
 #include <cstring>
+#include <initializer_list>
 #include <mutex>
 #include <numeric>
 #include <vector>
@@ -132,7 +133,8 @@ static int rho1_plan_build(Rho1Plan **out, const frpa_rho1_desc *D) {
                    D->i_valid_point_2_i_full_points_map[i], D->n_full_points - 1);
   // locality order (batches sharing basis functions together, largest first
   // within a key): the persistent kernel takes items in this order
-  rho1_fp64_build_items(batches, 64, 2, &items);
+  std::vector<int> chunk_items, chunk_batches;
+  rho1_fp64_build_items(batches, 64, 2, nb, &items, &chunk_items, &chunk_batches);
 
   Rho1Plan *P = new Rho1Plan();
   FRPA_CUDA_TRY(cudaGetDevice(&P->device));
@@ -147,6 +149,8 @@ static int rho1_plan_build(Rho1Plan **out, const frpa_rho1_desc *D) {
   P->n_valid_batches = n_valid_b;
   P->n_valid_points = n_valid_pts;
   P->wave_aligned16 = aligned;
+  P->fp64_chunk_items = chunk_items;
+  P->fp64_chunk_batches = chunk_batches;
   int st = FRPA_OK;
   auto up = [&](void **dst, const void *src, size_t bytes) {
     if (st != FRPA_OK) return;
@@ -204,6 +208,18 @@ static int rho1_plan_build(Rho1Plan **out, const frpa_rho1_desc *D) {
   return FRPA_OK;
 }
 
+// The kernels read the plan's 16-byte-load flag, which holds for the batch
+// offsets; wave pointers that are themselves less aligned lower it for the
+// duration of one launch (the plan is not copied: its host lists are large).
+struct WaveAlignGuard {
+  Rho1Plan &p;
+  int saved;
+  WaveAlignGuard(Rho1Plan &plan, const void *wave, const void *gwave) : p(plan), saved(plan.wave_aligned16) {
+    if (((uintptr_t)wave | (uintptr_t)gwave) & 15) p.wave_aligned16 = 0;
+  }
+  ~WaveAlignGuard() { p.wave_aligned16 = saved; }
+};
+
 static int rho1_run(Rho1Plan &P, int mode, int n_active, const double *wave, const double *gwave,
                     const double *P1, const double *bias, const double *gbias, double *rho, double *grad,
                     cudaStream_t stream) {
@@ -211,10 +227,9 @@ static int rho1_run(Rho1Plan &P, int mode, int n_active, const double *wave, con
   FRPA_CHECK_ARG(P.n_items == 0 || (wave && gwave), "rho1: null wave pointer");
   if (n_active > P.T) return fail(FRPA_ERR_INVALID, "rho1: j_atom_end - j_atom_begin + 1 = %d > ATOM_TILE_SIZE %d",
                                   n_active, P.T);
-  Rho1Plan Q = P;
-  if (((uintptr_t)wave | (uintptr_t)gwave) & 15) Q.wave_aligned16 = 0;
-  if (mode == FRPA_RHO1_FP64) return rho1_fp64_launch(Q, n_active, wave, gwave, P1, bias, gbias, rho, grad, stream);
-  if (mode == FRPA_RHO1_SPLIT_BF16) return rho1_split_launch(Q, n_active, wave, gwave, P1, bias, gbias, rho, grad, stream);
+  WaveAlignGuard aligned(P, wave, gwave);
+  if (mode == FRPA_RHO1_FP64) return rho1_fp64_launch(P, n_active, wave, gwave, P1, bias, gbias, rho, grad, stream);
+  if (mode == FRPA_RHO1_SPLIT_BF16) return rho1_split_launch(P, n_active, wave, gwave, P1, bias, gbias, rho, grad, stream);
   if (mode == FRPA_RHO1_SPLIT_I8) return rho1_i8_launch(P, n_active, wave, gwave, P1, bias, gbias, rho, grad, stream);
   return fail(FRPA_ERR_INVALID, "rho1: unknown mode %d", mode);
 }
@@ -269,6 +284,10 @@ struct Session {
   bool data = false;
   int device = 0;
   cudaStream_t stream = nullptr;
+  // the FP64 host-buffer entry copies the biases in and grad rho1 out chunk by
+  // chunk on these streams while the kernel works on the other chunks
+  cudaStream_t copy_in = nullptr, copy_out = nullptr;
+  cudaEvent_t ev_p1 = nullptr, ev_in[FP64_CHUNKS] = {}, ev_done[FP64_CHUNKS] = {};
   int T = 1;
   // rho1
   Rho1Plan *rho = nullptr;
@@ -299,6 +318,20 @@ void session_free_data(Session &S) {
   S.lhmfd = nullptr;
   S.mrs = S.opr = S.Q = S.spline = S.dv = nullptr;
   S.data = false;
+}
+
+void session_free_streams(Session &S) {
+  for (cudaStream_t *st : {&S.stream, &S.copy_in, &S.copy_out}) {
+    if (*st) cudaStreamDestroy(*st);
+    *st = nullptr;
+  }
+  if (S.ev_p1) cudaEventDestroy(S.ev_p1);
+  S.ev_p1 = nullptr;
+  for (int c = 0; c < FP64_CHUNKS; ++c) {
+    if (S.ev_in[c]) cudaEventDestroy(S.ev_in[c]);
+    if (S.ev_done[c]) cudaEventDestroy(S.ev_done[c]);
+    S.ev_in[c] = S.ev_done[c] = nullptr;
+  }
 }
 
 frpa_rho1_desc rho_desc_from_ref(int T, int *n_my_batches_work, int *n_full_points, int *n_basis,
@@ -465,9 +498,8 @@ int frpa_rho1_execute_fused_bias(const frpa_rho1_plan *plan, int n_active, int n
   FRPA_CHECK_ARG(j_coord >= 1 && j_coord <= 3, "rho1 fused bias: j_coord %d outside 1..3", j_coord);
   FRPA_CHECK_ARG(n_active == 0 || (j_atom_begin >= 1 && j_atom_begin + n_active - 1 <= n_atoms),
                  "rho1 fused bias: atoms %d..%d outside 1..%d", j_atom_begin, j_atom_begin + n_active - 1, n_atoms);
-  Rho1Plan Q = P;
-  if (((uintptr_t)wave | (uintptr_t)gradient_wave) & 15) Q.wave_aligned16 = 0;
-  return rho1_fp64_fused_bias_launch(Q, n_active, n_atoms, j_atom_begin, j_coord, atom_valid, density_matrix, wave,
+  WaveAlignGuard aligned(P, wave, gradient_wave);
+  return rho1_fp64_fused_bias_launch(P, n_active, n_atoms, j_atom_begin, j_coord, atom_valid, density_matrix, wave,
                                      gradient_wave, P1, bias, gbias, rho, grad, (cudaStream_t)stream);
 }
 
@@ -522,7 +554,8 @@ int frpa_rho1_plan_set_tuning(frpa_rho1_plan *plan, int key, int value) {
       return fail(FRPA_ERR_INVALID, "rho1 tuning: unknown key %d", key);
   }
   std::vector<Rho1WorkItem> items, split;
-  rho1_fp64_build_items(P.h_batches, P.fp64_tile_points, P.order, &items);
+  rho1_fp64_build_items(P.h_batches, P.fp64_tile_points, P.order, P.n_batches, &items, &P.fp64_chunk_items,
+                        &P.fp64_chunk_batches);
   rho1_split_build_items(P.h_batches, P.split_tile_points, P.order, &split);
   FRPA_TRY(replace_items(&P.d_items, &P.n_items, items));
   FRPA_TRY(replace_items(&P.d_items_split, &P.n_items_split, split));
@@ -911,7 +944,16 @@ void init_dfpt_device_info(void) {
          cudaGetErrorString(err));
     return;
   }
-  if (cudaSetDevice(dev) != cudaSuccess || cudaStreamCreateWithFlags(&S.stream, cudaStreamNonBlocking) != cudaSuccess) {
+  bool ok = cudaSetDevice(dev) == cudaSuccess &&
+            cudaStreamCreateWithFlags(&S.stream, cudaStreamNonBlocking) == cudaSuccess &&
+            cudaStreamCreateWithFlags(&S.copy_in, cudaStreamNonBlocking) == cudaSuccess &&
+            cudaStreamCreateWithFlags(&S.copy_out, cudaStreamNonBlocking) == cudaSuccess &&
+            cudaEventCreateWithFlags(&S.ev_p1, cudaEventDisableTiming) == cudaSuccess;
+  for (int c = 0; ok && c < FP64_CHUNKS; ++c)
+    ok = cudaEventCreateWithFlags(&S.ev_in[c], cudaEventDisableTiming) == cudaSuccess &&
+         cudaEventCreateWithFlags(&S.ev_done[c], cudaEventDisableTiming) == cudaSuccess;
+  if (!ok) {
+    session_free_streams(S);
     fail(FRPA_ERR_CUDA, "init_dfpt_device_info: stream creation failed");
     return;
   }
@@ -923,8 +965,7 @@ void free_dfpt_device_info(void) {
   std::lock_guard<std::mutex> lk(g_session_mu);
   Session &S = g_session;
   if (S.data) session_free_data(S);
-  if (S.stream) cudaStreamDestroy(S.stream);
-  S.stream = nullptr;
+  session_free_streams(S);
   S.info = false;
 }
 
@@ -1060,6 +1101,64 @@ int frpa_session_rho1_device_outputs(double **rho, double **grad) {
   return FRPA_OK;
 }
 
+// The session's FP64 step with host buffers, chunk by chunk: P1 goes in first,
+// the biases follow chunk by chunk on copy_in, the kernel runs one chunk of
+// batches after another on the session stream, and each finished chunk's
+// grad rho1 goes out on copy_out while the next chunk computes; rho1 (scattered
+// over all points) goes out last. Results are identical to one launch (every
+// work item computes the same way). All three streams are idle on return.
+static int rho1_session_chunked(Session &S, int n_active, const double *hP1, const double *hbias,
+                                const double *hgbias, double *hrho, double *hgrad) {
+  Rho1Plan &P = *S.rho;
+  if (n_active > P.T)
+    return fail(FRPA_ERR_INVALID, "rho1: j_atom_end - j_atom_begin + 1 = %d > ATOM_TILE_SIZE %d", n_active, P.T);
+  const int T = S.T, nb = S.n_batches;
+  const size_t nmb = (size_t)S.n_max_batch_size, nbias = nmb * nb * T, nrho = (size_t)S.n_full_points * T;
+  cudaStream_t s = S.stream, ci = S.copy_in, co = S.copy_out;
+  WaveAlignGuard aligned(P, S.wave, S.gwave);
+  int st = FRPA_OK;
+  auto run = [&]() -> int {
+    FRPA_CUDA_TRY(cudaMemcpyAsync(S.P1, hP1, sizeof(double) * (size_t)S.n_basis * S.n_basis * T,
+                                  cudaMemcpyHostToDevice, s));
+    FRPA_CUDA_TRY(cudaEventRecord(S.ev_p1, s));
+    FRPA_CUDA_TRY(cudaStreamWaitEvent(ci, S.ev_p1, 0));  // the biases queue behind P1 on the link
+    for (int c = 0; c < FP64_CHUNKS; ++c) {
+      const size_t b0 = P.fp64_chunk_batches[c], b1 = P.fp64_chunk_batches[c + 1];
+      for (int t = 0; t < T && b1 > b0; ++t) {
+        const size_t off = nmb * (b0 + (size_t)nb * t), len = nmb * (b1 - b0);
+        FRPA_CUDA_TRY(cudaMemcpyAsync(S.bias + off, hbias + off, sizeof(double) * len, cudaMemcpyHostToDevice, ci));
+        FRPA_CUDA_TRY(cudaMemcpyAsync(S.gbias + 3 * off, hgbias + 3 * off, sizeof(double) * 3 * len,
+                                      cudaMemcpyHostToDevice, ci));
+      }
+      FRPA_CUDA_TRY(cudaEventRecord(S.ev_in[c], ci));
+    }
+    // evaluate_first_order_rho.cpp:113-114 zeroes both outputs first
+    FRPA_CUDA_TRY(cudaMemsetAsync(S.out_rho, 0, sizeof(double) * nrho, s));
+    FRPA_CUDA_TRY(cudaMemsetAsync(S.out_grad, 0, sizeof(double) * 3 * nbias, s));
+    for (int c = 0; c < FP64_CHUNKS; ++c) {
+      FRPA_CUDA_TRY(cudaStreamWaitEvent(s, S.ev_in[c], 0));
+      FRPA_TRY(rho1_fp64_launch_chunk(P, c, n_active, S.wave, S.gwave, S.P1, S.bias, S.gbias, S.out_rho, S.out_grad,
+                                      s));
+      FRPA_CUDA_TRY(cudaEventRecord(S.ev_done[c], s));
+      FRPA_CUDA_TRY(cudaStreamWaitEvent(co, S.ev_done[c], 0));
+      const size_t b0 = P.fp64_chunk_batches[c], b1 = P.fp64_chunk_batches[c + 1];
+      for (int t = 0; t < T && b1 > b0; ++t) {
+        const size_t off = 3 * nmb * (b0 + (size_t)nb * t), len = 3 * nmb * (b1 - b0);
+        FRPA_CUDA_TRY(cudaMemcpyAsync(hgrad + off, S.out_grad + off, sizeof(double) * len, cudaMemcpyDeviceToHost, co));
+      }
+    }
+    FRPA_CUDA_TRY(cudaMemcpyAsync(hrho, S.out_rho, sizeof(double) * nrho, cudaMemcpyDeviceToHost, s));
+    return FRPA_OK;
+  };
+  st = run();
+  // leave no copy of the caller's buffers in flight, whatever happened
+  for (cudaStream_t x : {s, ci, co}) {
+    const cudaError_t e = cudaStreamSynchronize(x);
+    if (e != cudaSuccess && st == FRPA_OK) st = fail(FRPA_ERR_CUDA, "rho1 cu_host: %s", cudaGetErrorString(e));
+  }
+  return st;
+}
+
 void evaluate_first_order_rho_reduce_memory_c_v3_batches_atoms_cu_host_(
     int *n_my_batches_work, int *j_atom_begin, int *j_atom_end, int *j_coord, int *n_full_points, int *n_basis,
     int *n_atoms, int *n_max_compute_ham, int *n_centers_basis_I, int *n_max_batch_size, int *batch_sizes,
@@ -1102,6 +1201,11 @@ void evaluate_first_order_rho_reduce_memory_c_v3_batches_atoms_cu_host_(
   const int T = S.T;
   const size_t nbias = (size_t)S.n_max_batch_size * S.n_batches * T, nrho = (size_t)S.n_full_points * T;
   cudaStream_t s = S.stream;
+  if (g_rho1_mode == FRPA_RHO1_FP64 && (int)S.rho->fp64_chunk_items.size() == FP64_CHUNKS + 1) {
+    rho1_session_chunked(S, *j_atom_end - *j_atom_begin + 1, first_order_density_matrix, first_order_rho_bias_part2,
+                         first_order_gradient_rho_bias_batches_atoms, first_order_rho, first_order_gradient_rho);
+    return;
+  }
   if (cudaMemcpyAsync(S.P1, first_order_density_matrix, sizeof(double) * (size_t)S.n_basis * S.n_basis * T,
                       cudaMemcpyHostToDevice, s) != cudaSuccess ||
       cudaMemcpyAsync(S.bias, first_order_rho_bias_part2, sizeof(double) * nbias, cudaMemcpyHostToDevice, s) !=

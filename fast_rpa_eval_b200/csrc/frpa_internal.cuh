@@ -189,6 +189,11 @@ struct Rho1Plan {
   int fp64_ctas_per_sm = 0;    // 0: as many as fit
   int split_tile_points = 128; // <= 128 points per split-BF16 work item
   int order = 2;               // 0: largest items first, 1: batch order, 2: locality key
+  // the FP64 work list in FP64_CHUNKS pieces of consecutive batches (equal
+  // cost): chunk c holds items [fp64_chunk_items[c], fp64_chunk_items[c + 1])
+  // of batches [fp64_chunk_batches[c], fp64_chunk_batches[c + 1]), so the
+  // host-buffer entry point can overlap copies with compute chunk by chunk
+  std::vector<int> fp64_chunk_items, fp64_chunk_batches;
   std::vector<Rho1WorkItem> h_batches;
   std::vector<int> h_ib;  // host copy of the compact basis lists
   // split-int8 path: work lists (built with the plan) and the scratch
@@ -210,12 +215,22 @@ struct Rho1Plan {
 // work-list order (0 largest first, 1 batch order, 2 locality key) and the key
 void rho1_order_items(std::vector<Rho1WorkItem> *items, int order);
 int rho1_locality_key(const int *ib, int nc);
-void rho1_fp64_build_items(const std::vector<Rho1WorkItem> &batches, int tile_points, int order,
-                           std::vector<Rho1WorkItem> *out);
+constexpr int FP64_CHUNKS = 4;
+// FP64 work items, chunk by chunk (FP64_CHUNKS ranges of consecutive batches
+// of about equal cost, n_batches = the caller's batch count), each chunk in
+// the given order; the chunk boundaries go to chunk_items / chunk_batches
+void rho1_fp64_build_items(const std::vector<Rho1WorkItem> &batches, int tile_points, int order, int n_batches,
+                           std::vector<Rho1WorkItem> *out, std::vector<int> *chunk_items,
+                           std::vector<int> *chunk_batches);
 
 int rho1_fp64_launch(const Rho1Plan &plan, int n_active, const double *wave, const double *gwave,
                      const double *P1, const double *bias, const double *gbias, double *rho, double *grad,
                      cudaStream_t stream);
+// The FP64 kernel over the items of one chunk only, without zeroing the
+// outputs (the caller zeroes them once before the first chunk).
+int rho1_fp64_launch_chunk(const Rho1Plan &plan, int chunk, int n_active, const double *wave, const double *gwave,
+                           const double *P1, const double *bias, const double *gbias, double *rho, double *grad,
+                           cudaStream_t stream);
 int rho1_fp64_grid(int device);
 int rho1_fp64_fused_bias_launch(const Rho1Plan &plan, int n_active, int n_atoms, int j_atom_begin, int j_coord,
                                 const int *atom_valid, const double *density_matrix, const double *wave,

@@ -426,17 +426,19 @@ int fp64_grid(int device, int ctas_per_sm) {
   return per_sm * n_sm;
 }
 
+// items [item0, item0 + n_items) of the plan's list; the cursor must be zero
 template <int BN, bool BIAS>
-int fp64_launch(const Rho1Plan &plan, int n_active, const double *wave, const double *gwave, const double *P1,
-                const double *bias, const double *gbias, double *rho, double *grad, const FusedBias *fused,
-                cudaStream_t stream) {
+int fp64_launch(const Rho1Plan &plan, int item0, int n_items, int n_active, const double *wave, const double *gwave,
+                const double *P1, const double *bias, const double *gbias, double *rho, double *grad,
+                const FusedBias *fused, cudaStream_t stream) {
   int grid = fp64_grid<BN, BIAS>(plan.device, plan.fp64_ctas_per_sm);
   if (grid <= 0) return fail(FRPA_ERR_CUDA, "rho1_fp64: occupancy query failed");
-  if (grid > plan.n_items) grid = plan.n_items;
+  if (grid > n_items) grid = n_items;
+  if (grid <= 0) return FRPA_OK;
   FusedBias fb{};
   if (fused) fb = *fused;
   rho1_fp64_kernel<BN, BIAS><<<grid, Fp64Shape<BN, BIAS>::THREADS, sizeof(Smem<BN>), stream>>>(
-      plan.d_items, plan.n_items, plan.d_counter, plan.d_ib, plan.d_map, plan.T, n_active, plan.n_basis,
+      plan.d_items + item0, n_items, plan.d_counter, plan.d_ib, plan.d_map, plan.T, n_active, plan.n_basis,
       plan.n_full_points, plan.n_max_batch_size, plan.n_batches, wave, gwave, P1, bias, gbias, rho, grad,
       plan.wave_aligned16, fb);
   FRPA_LAUNCH_CHECK();
@@ -465,12 +467,30 @@ static int fp64_run(const Rho1Plan &plan, int n_active, const double *wave, cons
   FRPA_CUDA_TRY(cudaMemsetAsync(plan.d_counter, 0, sizeof(int), stream));
   if (fused) {
     if (plan.fp64_tile_points == 128)
-      return fp64_launch<128, true>(plan, n_active, wave, gwave, P1, bias, gbias, rho, grad, fused, stream);
-    return fp64_launch<64, true>(plan, n_active, wave, gwave, P1, bias, gbias, rho, grad, fused, stream);
+      return fp64_launch<128, true>(plan, 0, plan.n_items, n_active, wave, gwave, P1, bias, gbias, rho, grad, fused,
+                                    stream);
+    return fp64_launch<64, true>(plan, 0, plan.n_items, n_active, wave, gwave, P1, bias, gbias, rho, grad, fused,
+                                 stream);
   }
   if (plan.fp64_tile_points == 128)
-    return fp64_launch<128, false>(plan, n_active, wave, gwave, P1, bias, gbias, rho, grad, nullptr, stream);
-  return fp64_launch<64, false>(plan, n_active, wave, gwave, P1, bias, gbias, rho, grad, nullptr, stream);
+    return fp64_launch<128, false>(plan, 0, plan.n_items, n_active, wave, gwave, P1, bias, gbias, rho, grad, nullptr,
+                                   stream);
+  return fp64_launch<64, false>(plan, 0, plan.n_items, n_active, wave, gwave, P1, bias, gbias, rho, grad, nullptr,
+                                stream);
+}
+
+int rho1_fp64_launch_chunk(const Rho1Plan &plan, int chunk, int n_active, const double *wave, const double *gwave,
+                           const double *P1, const double *bias, const double *gbias, double *rho, double *grad,
+                           cudaStream_t stream) {
+  if (chunk < 0 || chunk + 1 >= (int)plan.fp64_chunk_items.size())
+    return fail(FRPA_ERR_INVALID, "rho1_fp64: chunk %d outside the plan's %d", chunk,
+                (int)plan.fp64_chunk_items.size() - 1);
+  const int i0 = plan.fp64_chunk_items[chunk], n = plan.fp64_chunk_items[chunk + 1] - i0;
+  if (n <= 0) return FRPA_OK;
+  FRPA_CUDA_TRY(cudaMemsetAsync(plan.d_counter, 0, sizeof(int), stream));
+  if (plan.fp64_tile_points == 128)
+    return fp64_launch<128, false>(plan, i0, n, n_active, wave, gwave, P1, bias, gbias, rho, grad, nullptr, stream);
+  return fp64_launch<64, false>(plan, i0, n, n_active, wave, gwave, P1, bias, gbias, rho, grad, nullptr, stream);
 }
 
 int rho1_fp64_launch(const Rho1Plan &plan, int n_active, const double *wave, const double *gwave, const double *P1,
@@ -519,20 +539,44 @@ int rho1_locality_key(const int *ib, int nc) {
 }
 
 // Work items of <= tile_points points (a batch's points split evenly, widths a
-// multiple of 8), in the given order.
-void rho1_fp64_build_items(const std::vector<Rho1WorkItem> &batches, int tile_points, int order,
-                           std::vector<Rho1WorkItem> *out) {
-  out->clear();
-  for (const Rho1WorkItem &b : batches) {
-    if (b.np == 0) continue;
-    const int tiles = (b.np + tile_points - 1) / tile_points;
-    int w = (b.np + tiles - 1) / tiles;
-    w = std::min(tile_points, (w + 7) & ~7);
-    for (int p0 = 0; p0 < b.np; p0 += w)
-      out->push_back(Rho1WorkItem{b.batch, b.nc, b.np, p0, std::min(w, b.np - p0), b.ib_off, b.prefix, b.key,
-                                  b.wave_off});
+// multiple of 8), grouped into FP64_CHUNKS ranges of consecutive batches of
+// about equal cost (nc^2 np), each range in the given order.
+void rho1_fp64_build_items(const std::vector<Rho1WorkItem> &batches, int tile_points, int order, int n_batches,
+                           std::vector<Rho1WorkItem> *out, std::vector<int> *chunk_items,
+                           std::vector<int> *chunk_batches) {
+  // chunk boundaries in the caller's batch indices (batches are in that order)
+  double total = 0.0;
+  for (const Rho1WorkItem &b : batches) total += (double)b.nc * b.nc * b.np;
+  std::vector<int> bounds(FP64_CHUNKS + 1, n_batches);
+  bounds[0] = 0;
+  {
+    double run = 0.0;
+    int c = 1;
+    for (const Rho1WorkItem &b : batches) {
+      while (c < FP64_CHUNKS && run >= total * c / FP64_CHUNKS) bounds[c++] = b.batch;
+      run += (double)b.nc * b.nc * b.np;
+    }
+    for (; c < FP64_CHUNKS; ++c) bounds[c] = n_batches;
   }
-  rho1_order_items(out, order);
+  out->clear();
+  std::vector<int> item_bounds(FP64_CHUNKS + 1, 0);
+  for (int c = 0; c < FP64_CHUNKS; ++c) {
+    std::vector<Rho1WorkItem> part;
+    for (const Rho1WorkItem &b : batches) {
+      if (b.np == 0 || b.batch < bounds[c] || b.batch >= bounds[c + 1]) continue;
+      const int tiles = (b.np + tile_points - 1) / tile_points;
+      int w = (b.np + tiles - 1) / tiles;
+      w = std::min(tile_points, (w + 7) & ~7);
+      for (int p0 = 0; p0 < b.np; p0 += w)
+        part.push_back(Rho1WorkItem{b.batch, b.nc, b.np, p0, std::min(w, b.np - p0), b.ib_off, b.prefix, b.key,
+                                    b.wave_off});
+    }
+    rho1_order_items(&part, order);
+    out->insert(out->end(), part.begin(), part.end());
+    item_bounds[c + 1] = (int)out->size();
+  }
+  if (chunk_items) *chunk_items = item_bounds;
+  if (chunk_batches) *chunk_batches = bounds;
 }
 
 }  // namespace frpa

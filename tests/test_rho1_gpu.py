@@ -87,6 +87,33 @@ def test_rho1_session_cu_host_matches_oracle():
             assert normwise_rel(g.reshape(g_o.shape, order="F"), g_o) < TOL_FP64
 
 
+@pytest.mark.parametrize("nb,T,pinned", [(3, 1, False), (64, 2, False), (64, 2, True)])
+def test_rho1_session_chunks_equal_one_launch(nb, T, pinned):
+    """The host-buffer entry point runs the FP64 step in four batch chunks with
+    the bias uploads and grad rho1 downloads overlapped; its outputs equal one
+    plan launch bit for bit (3 batches leave a chunk empty; T = 2 splits every
+    copy per perturbation; pinned buffers take the asynchronous copy path)."""
+    import torch
+
+    p = synth.make_rho1_problem(T=T, seed=43, n_batches=nb, with_bias=True, extra_full_points=3)
+    r_d, g_d = rho1_device_run(_lib.Rho1Plan(p), p)
+
+    def host_buf(a):
+        a = np.ascontiguousarray(np.asarray(a, dtype=np.float64).ravel(order="F"))
+        return torch.from_numpy(a).pin_memory() if pinned else a
+
+    P1, bias, gbias = (host_buf(a) for a in (p.first_order_density_matrix, p.first_order_rho_bias_part2,
+                                             p.first_order_gradient_rho_bias))
+    rho = host_buf(np.full(p.n_full_points * T, 7.0))
+    grad = host_buf(np.full(3 * p.n_max_batch_size * p.n_my_batches_work * T, 7.0))
+    with _lib.Session(p) as s:
+        for _ in range(2):  # the second call reuses the session's streams and events
+            r, g = s.rho1(P1=P1, bias=bias, gbias=gbias, rho=rho, grad=grad)
+            r = np.asarray(r).reshape(r_d.shape, order="F")
+            g = np.asarray(g).reshape(g_d.shape, order="F")
+            assert np.array_equal(r, r_d) and np.array_equal(g, g_d)
+
+
 def test_rho1_rejects_bad_input_without_touching_the_gpu_state():
     p = synth.make_rho1_problem(T=1, seed=3, n_batches=8)
     p.i_basis_batches[0, 0] = p.n_basis + 5
