@@ -208,18 +208,6 @@ static int rho1_plan_build(Rho1Plan **out, const frpa_rho1_desc *D) {
   return FRPA_OK;
 }
 
-// The kernels read the plan's 16-byte-load flag, which holds for the batch
-// offsets; wave pointers that are themselves less aligned lower it for the
-// duration of one launch (the plan is not copied: its host lists are large).
-struct WaveAlignGuard {
-  Rho1Plan &p;
-  int saved;
-  WaveAlignGuard(Rho1Plan &plan, const void *wave, const void *gwave) : p(plan), saved(plan.wave_aligned16) {
-    if (((uintptr_t)wave | (uintptr_t)gwave) & 15) p.wave_aligned16 = 0;
-  }
-  ~WaveAlignGuard() { p.wave_aligned16 = saved; }
-};
-
 static int rho1_run(Rho1Plan &P, int mode, int n_active, const double *wave, const double *gwave,
                     const double *P1, const double *bias, const double *gbias, double *rho, double *grad,
                     cudaStream_t stream) {
@@ -227,7 +215,6 @@ static int rho1_run(Rho1Plan &P, int mode, int n_active, const double *wave, con
   FRPA_CHECK_ARG(P.n_items == 0 || (wave && gwave), "rho1: null wave pointer");
   if (n_active > P.T) return fail(FRPA_ERR_INVALID, "rho1: j_atom_end - j_atom_begin + 1 = %d > ATOM_TILE_SIZE %d",
                                   n_active, P.T);
-  WaveAlignGuard aligned(P, wave, gwave);
   if (mode == FRPA_RHO1_FP64) return rho1_fp64_launch(P, n_active, wave, gwave, P1, bias, gbias, rho, grad, stream);
   if (mode == FRPA_RHO1_SPLIT_BF16) return rho1_split_launch(P, n_active, wave, gwave, P1, bias, gbias, rho, grad, stream);
   if (mode == FRPA_RHO1_SPLIT_I8) return rho1_i8_launch(P, n_active, wave, gwave, P1, bias, gbias, rho, grad, stream);
@@ -498,7 +485,6 @@ int frpa_rho1_execute_fused_bias(const frpa_rho1_plan *plan, int n_active, int n
   FRPA_CHECK_ARG(j_coord >= 1 && j_coord <= 3, "rho1 fused bias: j_coord %d outside 1..3", j_coord);
   FRPA_CHECK_ARG(n_active == 0 || (j_atom_begin >= 1 && j_atom_begin + n_active - 1 <= n_atoms),
                  "rho1 fused bias: atoms %d..%d outside 1..%d", j_atom_begin, j_atom_begin + n_active - 1, n_atoms);
-  WaveAlignGuard aligned(P, wave, gradient_wave);
   return rho1_fp64_fused_bias_launch(P, n_active, n_atoms, j_atom_begin, j_coord, atom_valid, density_matrix, wave,
                                      gradient_wave, P1, bias, gbias, rho, grad, (cudaStream_t)stream);
 }
@@ -1115,7 +1101,6 @@ static int rho1_session_chunked(Session &S, int n_active, const double *hP1, con
   const int T = S.T, nb = S.n_batches;
   const size_t nmb = (size_t)S.n_max_batch_size, nbias = nmb * nb * T, nrho = (size_t)S.n_full_points * T;
   cudaStream_t s = S.stream, ci = S.copy_in, co = S.copy_out;
-  WaveAlignGuard aligned(P, S.wave, S.gwave);
   int st = FRPA_OK;
   auto run = [&]() -> int {
     FRPA_CUDA_TRY(cudaMemcpyAsync(S.P1, hP1, sizeof(double) * (size_t)S.n_basis * S.n_basis * T,

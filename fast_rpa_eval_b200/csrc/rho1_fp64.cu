@@ -437,10 +437,12 @@ int fp64_launch(const Rho1Plan &plan, int item0, int n_items, int n_active, cons
   if (grid <= 0) return FRPA_OK;
   FusedBias fb{};
   if (fused) fb = *fused;
+  // 16-byte loads need even batch offsets (the plan) and 16-byte aligned arrays
+  const int aligned16 = plan.wave_aligned16 && !(((uintptr_t)wave | (uintptr_t)gwave) & 15);
   rho1_fp64_kernel<BN, BIAS><<<grid, Fp64Shape<BN, BIAS>::THREADS, sizeof(Smem<BN>), stream>>>(
       plan.d_items + item0, n_items, plan.d_counter, plan.d_ib, plan.d_map, plan.T, n_active, plan.n_basis,
       plan.n_full_points, plan.n_max_batch_size, plan.n_batches, wave, gwave, P1, bias, gbias, rho, grad,
-      plan.wave_aligned16, fb);
+      aligned16, fb);
   FRPA_LAUNCH_CHECK();
   return FRPA_OK;
 }
