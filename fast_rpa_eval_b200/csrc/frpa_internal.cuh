@@ -189,8 +189,8 @@ struct Rho1Plan {
   int fp64_ctas_per_sm = 0;    // 0: as many as fit
   int split_tile_points = 128; // <= 128 points per split-BF16 work item
   int order = 2;               // 0: largest items first, 1: batch order, 2: locality key
-  // the FP64 work list in FP64_CHUNKS pieces of consecutive batches (equal
-  // cost): chunk c holds items [fp64_chunk_items[c], fp64_chunk_items[c + 1])
+  // the FP64 work list in FP64_CHUNKS pieces of consecutive batches (6%, 44%,
+  // 44%, 6% of the cost): chunk c holds items [fp64_chunk_items[c], fp64_chunk_items[c + 1])
   // of batches [fp64_chunk_batches[c], fp64_chunk_batches[c + 1]), so the
   // host-buffer entry point can overlap copies with compute chunk by chunk
   std::vector<int> fp64_chunk_items, fp64_chunk_batches;
@@ -217,8 +217,9 @@ void rho1_order_items(std::vector<Rho1WorkItem> *items, int order);
 int rho1_locality_key(const int *ib, int nc);
 constexpr int FP64_CHUNKS = 4;
 // FP64 work items, chunk by chunk (FP64_CHUNKS ranges of consecutive batches
-// of about equal cost, n_batches = the caller's batch count), each chunk in
-// the given order; the chunk boundaries go to chunk_items / chunk_batches
+// holding 6%, 44%, 44% and 6% of the cost, n_batches = the caller's batch
+// count), each chunk in the given order; the chunk boundaries go to
+// chunk_items / chunk_batches
 void rho1_fp64_build_items(const std::vector<Rho1WorkItem> &batches, int tile_points, int order, int n_batches,
                            std::vector<Rho1WorkItem> *out, std::vector<int> *chunk_items,
                            std::vector<int> *chunk_batches);

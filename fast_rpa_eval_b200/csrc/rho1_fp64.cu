@@ -541,21 +541,25 @@ int rho1_locality_key(const int *ib, int nc) {
 }
 
 // Work items of <= tile_points points (a batch's points split evenly, widths a
-// multiple of 8), grouped into FP64_CHUNKS ranges of consecutive batches of
-// about equal cost (nc^2 np), each range in the given order.
+// multiple of 8), grouped into FP64_CHUNKS ranges of consecutive batches, each
+// range in the given order.  The ranges hold 6%, 44%, 44% and 6% of the cost
+// (nc^2 np): the host-buffer entry waits for the first range's biases before
+// any compute and for the last range's outputs after it, so those are small.
 void rho1_fp64_build_items(const std::vector<Rho1WorkItem> &batches, int tile_points, int order, int n_batches,
                            std::vector<Rho1WorkItem> *out, std::vector<int> *chunk_items,
                            std::vector<int> *chunk_batches) {
   // chunk boundaries in the caller's batch indices (batches are in that order)
   double total = 0.0;
   for (const Rho1WorkItem &b : batches) total += (double)b.nc * b.nc * b.np;
+  static_assert(FP64_CHUNKS == 4, "cost split of the chunks");
+  const double split[FP64_CHUNKS + 1] = {0.0, 0.06, 0.50, 0.94, 1.0};
   std::vector<int> bounds(FP64_CHUNKS + 1, n_batches);
   bounds[0] = 0;
   {
     double run = 0.0;
     int c = 1;
     for (const Rho1WorkItem &b : batches) {
-      while (c < FP64_CHUNKS && run >= total * c / FP64_CHUNKS) bounds[c++] = b.batch;
+      while (c < FP64_CHUNKS && run >= total * split[c]) bounds[c++] = b.batch;
       run += (double)b.nc * b.nc * b.np;
     }
     for (; c < FP64_CHUNKS; ++c) bounds[c] = n_batches;
