@@ -242,7 +242,8 @@ class Rho1Plan:
 
     def set_tuning(self, **kw):
         """fp64_tile_points (64 | 128), fp64_ctas_per_sm (0..3),
-        split_tile_points (16..128), order (0 largest first | 1 batch order),
+        split_tile_points (16..128), order (0 largest first | 1 batch order |
+        2 locality order, the default),
         split_i8_scratch_mb (>= 1: packed-operand scratch per group of batches)."""
         for k, v in kw.items():
             check(lib().frpa_rho1_plan_set_tuning(self.handle, c_int(TUNINGS[k]), c_int(int(v))))
