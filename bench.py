@@ -512,6 +512,7 @@ def run_frpa(args, ranks: Ranks):
     from fast_rpa_eval_b200 import _lib, autotune
 
     torch.cuda.set_device(ranks.local)
+    _lib.set_device(ranks.local)  # the library's own runtime: plans and the session on this rank's GPU
     stream = torch.cuda.current_stream()
     peaks = measured_peaks()
     mode_name = args.mode or "fp64"

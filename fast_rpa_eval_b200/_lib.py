@@ -345,6 +345,19 @@ def set_atom_tile_size(T: int):
     check(lib().frpa_set_atom_tile_size(c_int(T)))
 
 
+def set_device(device: int):
+    """frpa_set_device: the GPU the library's own (static) CUDA runtime makes
+    current on this thread; plans and the session created afterwards use it.
+    Call it with torch's device when that is not device 0."""
+    check(lib().frpa_set_device(c_int(device)))
+
+
+def get_device() -> int:
+    d = c_int(-1)
+    check(lib().frpa_get_device(ctypes.byref(d)))
+    return d.value
+
+
 def set_rho1_mode(mode: int):
     check(lib().frpa_set_rho1_mode(c_int(mode)))
 

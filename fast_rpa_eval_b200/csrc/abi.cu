@@ -404,6 +404,18 @@ const char *frpa_last_error_message(void) { return t_msg; }
 void frpa_clear_error(void) { clear_error(); }
 int frpa_version(void) { return 10000; }
 
+int frpa_set_device(int device) {
+  int count = 0;
+  FRPA_CUDA_TRY(cudaGetDeviceCount(&count));
+  if (device < 0 || device >= count) return fail(FRPA_ERR_INVALID, "device %d outside 0..%d", device, count - 1);
+  FRPA_CUDA_TRY(cudaSetDevice(device));
+  return FRPA_OK;
+}
+int frpa_get_device(int *device) {
+  if (!device) return fail(FRPA_ERR_INVALID, "frpa_get_device: null argument");
+  FRPA_CUDA_TRY(cudaGetDevice(device));
+  return FRPA_OK;
+}
 int frpa_set_atom_tile_size(int T) {
   if (T < 1 || T > FRPA_MAX_ATOM_TILE) return fail(FRPA_ERR_INVALID, "atom tile size %d out of range", T);
   g_tile = T;
@@ -921,8 +933,12 @@ void init_dfpt_device_info(void) {
   clear_error();
   Session &S = g_session;
   if (S.info) return;
+  // $FRPA_DEVICE, else the library's current device (frpa_set_device; 0 unless set)
   int dev = 0;
-  if (const char *e = getenv("FRPA_DEVICE")) dev = atoi(e);
+  if (const char *e = getenv("FRPA_DEVICE"))
+    dev = atoi(e);
+  else if (cudaGetDevice(&dev) != cudaSuccess)
+    dev = 0;
   int count = 0;
   cudaError_t err = cudaGetDeviceCount(&count);
   if (err != cudaSuccess || dev < 0 || dev >= count) {

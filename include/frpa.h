@@ -54,6 +54,15 @@ const char *frpa_last_error_message(void);
 void frpa_clear_error(void);
 int frpa_version(void);
 
+/* The GPU that plans and the session created afterwards on this thread use:
+ * cudaSetDevice in the library's own CUDA runtime (it is linked statically, so
+ * a caller's cudaSetDevice through another runtime need not reach it).  The
+ * session (init_dfpt_device_info) takes $FRPA_DEVICE if set, else this device,
+ * which is device 0 unless set -- the reference's fixed choice
+ * (device.cu:7-9).  No counterpart in the reference. */
+int frpa_set_device(int device);
+int frpa_get_device(int *device);
+
 /* ATOM_TILE_SIZE for the reference drop-ins (setting.h:19-21), 1..64. */
 int frpa_set_atom_tile_size(int T);
 int frpa_get_atom_tile_size(void);

@@ -114,6 +114,18 @@ def test_rho1_session_chunks_equal_one_launch(nb, T, pinned):
             assert np.array_equal(r, r_d) and np.array_equal(g, g_d)
 
 
+def test_library_device_selection():
+    """frpa_set_device drives the library's own CUDA runtime (the one plans and
+    the session use); a device past the last is rejected with a message."""
+    import torch
+
+    _lib.set_device(torch.cuda.current_device())
+    assert _lib.get_device() == torch.cuda.current_device()
+    with pytest.raises(_lib.FrpaError, match="outside"):
+        _lib.set_device(torch.cuda.device_count())
+    assert _lib.get_device() == torch.cuda.current_device()
+
+
 def test_rho1_rejects_bad_input_without_touching_the_gpu_state():
     p = synth.make_rho1_problem(T=1, seed=3, n_batches=8)
     p.i_basis_batches[0, 0] = p.n_basis + 5
