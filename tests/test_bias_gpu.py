@@ -120,3 +120,30 @@ def test_fused_bias_equals_rho1_plus_bias_part2(j_coord):
     assert rel(got, want) < TOL
     assert np.array_equal(got[:, 3], want[:, 3])  # perturbation 4 is not active
     assert torch.equal(grad, grad0)
+
+
+@pytest.mark.gpu
+def test_fused_bias_same_bits_for_both_tile_widths():
+    """The fused-bias launch at 128-point work items (the FP64 tile tuning)
+    gives the same bits as at 64-point items: per point, both sum the row
+    tiles and the lanes of a warp in the same order."""
+    import torch
+
+    from gpu_util import dev
+
+    p = synth.make_rho1_problem(T=2, seed=19, n_atoms=6, n_batches=20, with_bias=True, np_range=(60, 250))
+    dm = np.random.default_rng(6).normal(size=(p.n_basis, p.n_basis))
+    plan = _lib.Rho1Plan(p)
+    args = [dev(p.wave), dev(p.gradient_wave), dev(p.first_order_density_matrix), dev(p.first_order_rho_bias_part2),
+            dev(p.first_order_gradient_rho_bias)]
+    n_rho, n_grad = p.n_full_points * 2, 3 * p.n_max_batch_size * p.n_my_batches_work * 2
+    outs = []
+    for tile in (64, 128):
+        plan.set_tuning(fp64_tile_points=tile)
+        rho, grad = (torch.zeros(n, dtype=torch.float64, device="cuda") for n in (n_rho, n_grad))
+        plan.execute_fused_bias(2, p.n_atoms, 1, 1, dev(p.atom_valid_n_compute_c_batches, np.int32), dev(dm), *args,
+                                rho, grad)
+        torch.cuda.synchronize()
+        outs.append((rho, grad))
+    assert plan.device_flags() == 0
+    assert torch.equal(outs[0][0], outs[1][0]) and torch.equal(outs[0][1], outs[1][1])
