@@ -38,6 +38,7 @@
 #include <cmath>
 #include <cstring>
 #include <mutex>
+#include <utility>
 #include <vector>
 
 #include "frpa_internal.cuh"
@@ -58,9 +59,6 @@ __constant__ double c_Kcos[SU_LMAX + 1][SU_LMAX + 1];
 __constant__ double c_RA[SU_LMAX + 1][SU_LMAX + 1];
 __constant__ double c_RB[SU_LMAX + 1][SU_LMAX + 1];
 __constant__ double c_DF[SU_LMAX + 1];
-// exponents (a, b, c) of each graded Kelvin slot, for the adjoint
-__constant__ int c_kabc[3][kelvin_count(SU_LMAX)];
-
 __host__ __device__ constexpr int n_kelvin(int L) { return kelvin_count(L); }
 
 // record layout (doubles) for one (centre slot, t)
@@ -468,74 +466,123 @@ int launch_fast(const SumupPlan &P, int n_active, const double *spline, double *
 
 constexpr int ADJ_KCH = 32;
 
+// Exponents (a, b, c) of coefficient slot k in the degree-graded packing
+// (the inverse of kelvin_index), for compile-time use.
+struct Abc {
+  int a, b, c;
+};
+__host__ __device__ constexpr Abc kelvin_abc(int k) {
+  int d = 0;
+  while ((d + 1) * (d + 2) * (d + 3) / 6 <= k) ++d;
+  int r = k - d * (d + 1) * (d + 2) / 6, a = 0;
+  while (r >= d + 1 - a) {
+    r -= d + 1 - a;
+    ++a;
+  }
+  return Abc{a, r, d - a - r};
+}
+__host__ __device__ constexpr bool kelvin_abc_inverts_index() {
+  for (int k = 0; k < kelvin_count(SU_LMAX); ++k) {
+    const Abc m = kelvin_abc(k);
+    if (kelvin_index(m.a, m.b, m.c) != k) return false;
+  }
+  return true;
+}
+static_assert(kelvin_abc_inverts_index(), "kelvin_abc is the inverse of kelvin_index");
+
+// acc[I] += w ux^a uy^b uz^c for the chunk's slots K0 + I of degree <= lam
+// (exponents are compile-time constants: the power arrays stay in registers)
+template <int L, int K0, int... I>
+__device__ __forceinline__ void dcoef_terms(std::integer_sequence<int, I...>, double *acc, double w, const double *pa,
+                                            const double *pb, const double *pc, int lam) {
+  auto term = [&](auto ic) {
+    constexpr int k = K0 + decltype(ic)::value;
+    if constexpr (k < kelvin_count(L)) {
+      constexpr Abc m = kelvin_abc(k);
+      if (m.a + m.b + m.c <= lam) acc[decltype(ic)::value] += w * pa[m.a] * pb[m.b] * pc[m.c];
+    }
+  };
+  (term(std::integral_constant<int, I>{}), ...);
+}
+
+// One chunk of ADJ_KCH coefficient slots starting at K0: every point of the
+// block once, then the block's partial sums (warp shuffles, then the warps in
+// order) to part[k, slot, t, z].
+template <int L, int K0>
+__device__ __forceinline__ void dcoef_chunk(int n_full, const int *__restrict__ map,
+                                            const double *__restrict__ coord, const double *__restrict__ rec,
+                                            const double *__restrict__ g, int t, int p_begin, int p_end,
+                                            double (&red)[SU_THREADS / 32][ADJ_KCH], double *__restrict__ part) {
+  const double cx = rec[R_X], cy = rec[R_Y], cz = rec[R_Z], mrs = rec[R_MRS];
+  const int lam0 = (int)rec[R_LAM0];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  double acc[ADJ_KCH];
+#pragma unroll
+  for (int kk = 0; kk < ADJ_KCH; ++kk) acc[kk] = 0.0;
+  for (int iv = p_begin + threadIdx.x; iv < p_end; iv += SU_THREADS) {
+    const int f = map[iv];
+    const double dx = sub_rn(coord[3LL * f], cx), dy = sub_rn(coord[3LL * f + 1], cy),
+                 dz = sub_rn(coord[3LL * f + 2], cz);
+    const double d2 = add_rn(add_rn(mul_rn(dx, dx), mul_rn(dy, dy)), mul_rn(dz, dz));
+    if (d2 < mrs || !(d2 < 1e8)) continue;
+    int lam = lam0;
+    while (rec[R_OPR + lam] < d2 && lam > 0) --lam;
+    const double ri = rsqrt(d2), ir2 = ri * ri;
+    const double ux = dx * ir2, uy = dy * ir2, uz = dz * ir2;
+    double pa[L + 1], pb[L + 1], pc[L + 1];
+    pa[0] = pb[0] = pc[0] = 1.0;
+#pragma unroll
+    for (int e = 1; e <= L; ++e) {
+      pa[e] = pa[e - 1] * ux;
+      pb[e] = pb[e - 1] * uy;
+      pc[e] = pc[e - 1] * uz;
+    }
+    const double w = g[f + (long long)n_full * t] * ri;
+    dcoef_terms<L, K0>(std::make_integer_sequence<int, ADJ_KCH>{}, acc, w, pa, pb, pc, lam);
+  }
+#pragma unroll
+  for (int kk = 0; kk < ADJ_KCH; ++kk) {
+    double v = acc[kk];
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
+    if (lane == 0) red[warp][kk] = v;
+  }
+  __syncthreads();
+  constexpr int NK = kelvin_count(L);
+  if (threadIdx.x < ADJ_KCH && K0 + (int)threadIdx.x < NK) {
+    double v = 0.0;
+    for (int w = 0; w < SU_THREADS / 32; ++w) v += red[w][threadIdx.x];
+    part[K0 + threadIdx.x] = v;  // this point block's partial, summed over the blocks in order later
+  }
+  __syncthreads();
+}
+
+template <int L, int... C>
+__device__ __forceinline__ void dcoef_chunks(std::integer_sequence<int, C...>, int n_full, const int *map,
+                                             const double *coord, const double *rec, const double *g, int t,
+                                             int p_begin, int p_end, double (&red)[SU_THREADS / 32][ADJ_KCH],
+                                             double *part) {
+  (dcoef_chunk<L, C * ADJ_KCH>(n_full, map, coord, rec, g, t, p_begin, p_end, red, part), ...);
+}
+
 // part[k, slot, t, z] = sum over point block z's points of g(p, t) u^k / r
 // for far-field pairs with deg(k) <= lam (the derivative of the fast path's
-// Horner sum with respect to its coefficients); each block sums its points in
-// a fixed order, and sumup_dcoef_reduce_kernel adds the blocks in order, so
-// the result is the same on every run.
+// Horner sum with respect to its coefficients), one instance per l_max; each
+// block sums its points in a fixed order, and sumup_dcoef_reduce_kernel adds
+// the blocks in order, so the result is the same on every run.
+template <int L>
 __global__ void __launch_bounds__(SU_THREADS)
     sumup_dcoef_kernel(int n_valid, int n_full, const int *__restrict__ map, const double *__restrict__ coord,
-                       int n_chp, int L, const double *__restrict__ recs, const double *__restrict__ g,
-                       int pts_per_block, double *__restrict__ dcoef) {
-  const int RS = rec_stride(L);
-  const int NK = n_kelvin(L);
+                       int n_chp, const double *__restrict__ recs, const double *__restrict__ g, int pts_per_block,
+                       double *__restrict__ dcoef) {
+  constexpr int NK = kelvin_count(L), NCH = (NK + ADJ_KCH - 1) / ADJ_KCH;
   __shared__ double red[SU_THREADS / 32][ADJ_KCH];
   const int slot = blockIdx.x, t = blockIdx.y;
   const int p_begin = blockIdx.z * pts_per_block;
   const int p_end = min(n_valid, p_begin + pts_per_block);
-  const double *rec = recs + (long long)RS * (slot + (long long)n_chp * t);
-  const double cx = rec[R_X], cy = rec[R_Y], cz = rec[R_Z], mrs = rec[R_MRS];
-  const int lam0 = (int)rec[R_LAM0];
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-#pragma unroll 1
-  for (int k0 = 0; k0 < NK; k0 += ADJ_KCH) {
-    double acc[ADJ_KCH];
-#pragma unroll
-    for (int kk = 0; kk < ADJ_KCH; ++kk) acc[kk] = 0.0;
-    for (int iv = p_begin + threadIdx.x; iv < p_end; iv += SU_THREADS) {
-      const int f = map[iv];
-      const double dx = sub_rn(coord[3LL * f], cx), dy = sub_rn(coord[3LL * f + 1], cy),
-                   dz = sub_rn(coord[3LL * f + 2], cz);
-      const double d2 = add_rn(add_rn(mul_rn(dx, dx), mul_rn(dy, dy)), mul_rn(dz, dz));
-      if (d2 < mrs || !(d2 < 1e8)) continue;
-      int lam = lam0;
-      while (rec[R_OPR + lam] < d2 && lam > 0) --lam;
-      const double ri = rsqrt(d2), ir2 = ri * ri;
-      const double ux = dx * ir2, uy = dy * ir2, uz = dz * ir2;
-      double pa[SU_LMAX + 1], pb[SU_LMAX + 1], pc[SU_LMAX + 1];
-      pa[0] = pb[0] = pc[0] = 1.0;
-#pragma unroll
-      for (int e = 1; e <= SU_LMAX; ++e) {
-        pa[e] = pa[e - 1] * ux;
-        pb[e] = pb[e - 1] * uy;
-        pc[e] = pc[e - 1] * uz;
-      }
-      const double w = g[f + (long long)n_full * t] * ri;
-#pragma unroll
-      for (int kk = 0; kk < ADJ_KCH; ++kk) {
-        const int k = k0 + kk;
-        if (k < NK) {
-          const int a = c_kabc[0][k], b = c_kabc[1][k], c = c_kabc[2][k];
-          if (a + b + c <= lam) acc[kk] += w * pa[a] * pb[b] * pc[c];
-        }
-      }
-    }
-#pragma unroll
-    for (int kk = 0; kk < ADJ_KCH; ++kk) {
-      double v = acc[kk];
-#pragma unroll
-      for (int off = 16; off > 0; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
-      if (lane == 0) red[warp][kk] = v;
-    }
-    __syncthreads();
-    if (threadIdx.x < ADJ_KCH && k0 + threadIdx.x < NK) {
-      double v = 0.0;
-      for (int w = 0; w < SU_THREADS / 32; ++w) v += red[w][threadIdx.x];
-      // this point block's partial, summed over the blocks in order later
-      dcoef[(k0 + threadIdx.x) + (long long)NK * (slot + (long long)n_chp * (t + (long long)gridDim.y * blockIdx.z))] = v;
-    }
-    __syncthreads();
-  }
+  const double *rec = recs + (long long)rec_stride(L) * (slot + (long long)n_chp * t);
+  double *part = dcoef + (long long)NK * (slot + (long long)n_chp * (t + (long long)gridDim.y * blockIdx.z));
+  dcoef_chunks<L>(std::make_integer_sequence<int, NCH>{}, n_full, map, coord, rec, g, t, p_begin, p_end, red, part);
 }
 
 // dcoef[k, slot, t] = sum over the point blocks z, in order, of part[k, slot, t, z]
@@ -591,8 +638,19 @@ __global__ void sumup_dq_kernel(int n_atoms, int L, int L2, int mc_dim, int icc_
 
 int launch_dcoef(const SumupPlan &P, int n_active, const double *g, cudaStream_t stream) {
   const dim3 grid(P.n_chp, n_active, P.adj_nz);
-  sumup_dcoef_kernel<<<grid, SU_THREADS, 0, stream>>>(P.n_valid_points, P.n_full_points, P.d_map, P.d_coord,
-                                                       P.n_chp, P.L, P.d_recs, g, P.adj_pts, P.d_dcoef_part);
+  switch (P.L) {
+#define FRPA_DCOEF_CASE(LL)                                                                                  \
+  case LL:                                                                                                   \
+    sumup_dcoef_kernel<LL><<<grid, SU_THREADS, 0, stream>>>(P.n_valid_points, P.n_full_points, P.d_map,       \
+                                                             P.d_coord, P.n_chp, P.d_recs, g, P.adj_pts,       \
+                                                             P.d_dcoef_part);                                  \
+    break;
+    FRPA_DCOEF_CASE(0) FRPA_DCOEF_CASE(1) FRPA_DCOEF_CASE(2) FRPA_DCOEF_CASE(3) FRPA_DCOEF_CASE(4)
+    FRPA_DCOEF_CASE(5) FRPA_DCOEF_CASE(6) FRPA_DCOEF_CASE(7) FRPA_DCOEF_CASE(8)
+#undef FRPA_DCOEF_CASE
+    default:
+      return fail(FRPA_ERR_UNSUPPORTED, "sum-up adjoint: l_pot_max %d above %d", P.L, SU_LMAX);
+  }
   FRPA_LAUNCH_CHECK();
   const long long n = (long long)P.n_coef * P.n_chp * n_active;
   sumup_dcoef_reduce_kernel<<<(int)std::min<long long>(4096, (n + 255) / 256), 256, 0, stream>>>(
@@ -638,16 +696,6 @@ static int sumup_upload_constants_once() {
   FRPA_CUDA_TRY(cudaMemcpyToSymbol(c_RA, RA, sizeof(RA)));
   FRPA_CUDA_TRY(cudaMemcpyToSymbol(c_RB, RB, sizeof(RB)));
   FRPA_CUDA_TRY(cudaMemcpyToSymbol(c_DF, DF, sizeof(DF)));
-  int kabc[3][kelvin_count(SU_LMAX)] = {};
-  for (int a = 0; a <= SU_LMAX; ++a)
-    for (int b = 0; a + b <= SU_LMAX; ++b)
-      for (int c = 0; a + b + c <= SU_LMAX; ++c) {
-        const int k = kelvin_index(a, b, c);
-        kabc[0][k] = a;
-        kabc[1][k] = b;
-        kabc[2][k] = c;
-      }
-  FRPA_CUDA_TRY(cudaMemcpyToSymbol(c_kabc, kabc, sizeof(kabc)));
   return FRPA_OK;
 }
 
