@@ -44,6 +44,8 @@ namespace frpa {
 namespace {
 
 constexpr int BM = 64, BN = 64, KC = 16, THREADS = 256;
+constexpr int COEF_PTS = 128;  // points whose coefficients are staged together (a multiple of KC)
+static_assert(COEF_PTS % KC == 0, "coefficient stage holds whole K chunks");
 constexpr int LDA = BM + 4;  // As[k = point][m = i]
 constexpr int LDB = KC + 4;  // Bs[n = j][k = point]
 constexpr int EMAX_EMPTY = -2139062144;  // 0x80808080: no non-zero bound seen
@@ -263,7 +265,7 @@ __global__ void __launch_bounds__(THREADS, 2) h1_tile_kernel(const H1Item *__res
   __shared__ __align__(16) double Bs[BN * LDB];  // phi(n0 + n, k)
   __shared__ __align__(16) double Ps[SYM ? KC * LDA : 1];  // phi(m0 + m, k)
   __shared__ __align__(16) double Qs[SYM ? BN * LDB : 1];  // A(n0 + n, k)
-  __shared__ PointCoef coef[KC];
+  __shared__ PointCoef coef[COEF_PTS];  // the per-point coefficients of COEF_PTS points at a time
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int wm = warp >> 2, wn = warp & 3, g = lane >> 2, q = lane & 3;
   const long long nb2 = (long long)a.n_basis * a.n_basis;
@@ -288,7 +290,9 @@ __global__ void __launch_bounds__(THREADS, 2) h1_tile_kernel(const H1Item *__res
       for (int y = 0; y < 2; ++y) acc[x][y][0] = acc[x][y][1] = 0.0;
 
     for (int k0 = 0; k0 < np; k0 += KC) {
-      if (tid < KC && k0 + tid < np) coef[tid] = point_coef(a, W.batch, k0 + tid, W.prefix, t);
+      if (k0 % COEF_PTS == 0) {  // every thread, one point each (the loads of many points in flight)
+        for (int e = tid; e < COEF_PTS && k0 + e < np; e += THREADS) coef[e] = point_coef(a, W.batch, k0 + e, W.prefix, t);
+      }
       __syncthreads();
       {
         // thread -> one point k of the chunk and four consecutive rows: the
@@ -297,7 +301,7 @@ __global__ void __launch_bounds__(THREADS, 2) h1_tile_kernel(const H1Item *__res
         const int k = tid / (BM / RPT), r0 = (tid % (BM / RPT)) * RPT, p = k0 + k;
         const bool pok = p < np;
         const long long pc = (long long)(pok ? p : 0) * ncp;
-        const PointCoef c = coef[k];
+        const PointCoef c = coef[(k0 % COEF_PTS) + k];
         const int jc = a.mode == 1 ? a.h.j_coord : 1;
         const double *ph = phi + pc, *gp = gph + 3 * pc, *hp = hph ? hph + 6 * pc : nullptr;
 #pragma unroll
